@@ -1,0 +1,395 @@
+"""Benchmark of the Roe-Exner SSPRK2 step on B200 (one JSON line on stdout, rank 0).
+
+Workload (default): the Gaussian-bed Roe-Exner case, 2048 x 2048 cells (+ ring),
+dx = 0.01 m, MPM bedload, Transmissive x / Reflective y, CFL 0.5, SSPRK2, float32 —
+the configuration the metric is quoted on.  A step is one full SSPRK2 step (CFL
+reduction + two fused stage kernels) over every physical cell; one cell advanced by one
+step is one cell-update.
+
+Reported:
+  value      cell-updates/s of the device loop (graph replay), state resident in HBM,
+             L2 flushed (256 MiB write) between timed steps and excluded from the timing;
+  e2e        the same metric through the public API with host buffers: pinned-host ->
+             device copy of the state, ``run_steps`` for all K steps, device -> host copy
+             of the state, all inside the timed region;
+  roofline   the stage kernels' algorithmic bytes per launch over their CUDA-event
+             duration, against the measured HBM copy bandwidth;
+  fp64       the same loop in float64 (the plain FP64 GPU path) and its speed ratio;
+  accuracy   rel-L1 of h and z+z_b, float32 vs float64 after the accuracy run;
+  cpu_baseline  the float64 NumPy oracle on a bounded sample on the host cores.
+
+``--impl reference`` times the reference algorithm on the CPU instead (the float64
+oracle restatement of PyExner's JAX step; JAX itself is not installed on these hosts)
+and prints its line with "impl": "reference".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s Roe-Exner SSPRK2 FP32 vs FP64 at stated L1 err; % HBM peak"
+UNIT = "cell-updates/s"
+# algorithmic words per cell per launch (Measurement)
+WORDS_STAGE1 = 10   # reads h hu hv z_b z n_b, writes h hu hv z_b
+WORDS_STAGE2 = 16   # reads h hu hv z_b z n_b + u^n h hu hv z_b G, writes h hu hv z_b G
+WORDS_CFL = 4       # reads h hu hv G
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            parts = [p.strip() for p in l.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def build_case(n, dtype, device):
+    import torch
+
+    from pyexner_b200 import RoeExnerState, cases, create_solver_bundle
+
+    c = cases.gaussian_bed(n, device=device)
+    st = RoeExnerState.from_numpy(c["arrs"], c["seds"], dtype)
+    bundle = create_solver_bundle("Roe Exner")
+    cfg = bundle.config(st, None, c["boundaries"], c["dx"], c["params"])
+    mask = bundle.mask_fn(st, None, c["boundaries"].boundary_mask)
+    st = bundle.init_fn(st, mask, cfg)
+    torch.cuda.synchronize()
+    return c, bundle, cfg, mask, st
+
+
+def timed_device_loop(st, mask, cfg, steps, warmup, flush):
+    """Graph-replayed SSPRK2 steps, one step per timed interval, L2 flushed between."""
+    import torch
+
+    from pyexner_b200 import run_steps
+    from pyexner_b200.integrators import check_state, scratch_like
+
+    b = scratch_like(st)
+    run_steps(st, mask, cfg, "SSPRK2", warmup, 0.5, scratch=b)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    total = 0.0
+    for _ in range(steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        run_steps(st, mask, cfg, "SSPRK2", 1, 0.5, scratch=b, log_dt=False)
+        e1.record(stream)
+        e1.synchronize()
+        total += e0.elapsed_time(e1) / 1e3
+    check_state(st, mask, cfg)
+    return total, b
+
+
+def kernel_breakdown(st, b, mask, cfg, steps, flush):
+    """CUDA-event duration of each kernel (CFL, stage 1, stage 2) over ``steps`` steps."""
+    import ctypes
+
+    import torch
+
+    from pyexner_b200 import _lib
+    from pyexner_b200.solvers import _re_plan, _stream
+
+    plan = _re_plan(st, mask, cfg)
+    dt = torch.empty((), dtype=st.dtype, device=st.h.device)
+    stream = torch.cuda.current_stream()
+    A = st.c_fields()
+    B1 = b.c_fields()
+    B1.G = None
+    B1.z = st.z.data_ptr()
+    B1.n_b = st.n_b.data_ptr()
+    B2 = b.c_fields()
+    B2.z = st.z.data_ptr()
+    B2.n_b = st.n_b.data_ptr()
+    acc = {"cfl": 0.0, "stage1": 0.0, "stage2": 0.0}
+    for _ in range(steps):
+        flush.zero_()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev[0].record(stream)
+        _lib.call("pxb_re_cfl", plan.handle, ctypes.byref(A), 0.5, ctypes.c_void_p(dt.data_ptr()), _stream())
+        ev[1].record(stream)
+        _lib.call("pxb_re_stage", plan.handle, ctypes.byref(A), ctypes.byref(B1), None,
+                  ctypes.c_void_p(dt.data_ptr()), _stream())
+        ev[2].record(stream)
+        _lib.call("pxb_re_stage", plan.handle, ctypes.byref(B2), ctypes.byref(A), ctypes.byref(A),
+                  ctypes.c_void_p(dt.data_ptr()), _stream())
+        ev[3].record(stream)
+        ev[3].synchronize()
+        acc["cfl"] += ev[0].elapsed_time(ev[1]) / 1e3
+        acc["stage1"] += ev[1].elapsed_time(ev[2]) / 1e3
+        acc["stage2"] += ev[2].elapsed_time(ev[3]) / 1e3
+    return {k: v / steps for k, v in acc.items()}
+
+
+def e2e_run(n, dtype, steps, warmup):
+    """Host buffers in, host buffers out, through the public API."""
+    import torch
+
+    from pyexner_b200 import RoeExnerState, cases, create_solver_bundle, run_steps
+
+    c = cases.gaussian_bed(n, device="cuda")
+    planes = ("h", "hu", "hv", "z", "z_b", "n", "G")
+    host = {k: torch.from_numpy(np.ascontiguousarray(c["arrs"][k])).to(dtype).pin_memory() for k in planes}
+    out = {k: torch.empty_like(host[k]).pin_memory() for k in ("h", "hu", "hv", "z_b", "G")}
+    st = RoeExnerState.from_numpy(c["arrs"], c["seds"], dtype)
+    bundle = create_solver_bundle("Roe Exner")
+    cfg = bundle.config(st, None, c["boundaries"], c["dx"], c["params"])
+    mask = bundle.mask_fn(st, None, c["boundaries"].boundary_mask)
+    st = bundle.init_fn(st, mask, cfg)
+    run_steps(st, mask, cfg, "SSPRK2", warmup, 0.5)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in planes:
+        getattr(st, k).copy_(host[k], non_blocking=True)
+    st2 = bundle.init_fn(st, mask, cfg)
+    run_steps(st2, mask, cfg, "SSPRK2", steps, 0.5, log_dt=False)
+    for k in out:
+        out[k].copy_(getattr(st2, k), non_blocking=True)
+    e1.record(stream)
+    e1.synchronize()
+    sec = e0.elapsed_time(e1) / 1e3
+    h2d = sum(v.numel() * v.element_size() for v in host.values())
+    d2h = sum(v.numel() * v.element_size() for v in out.values())
+    return sec, h2d, d2h
+
+
+def accuracy_run(n, steps):
+    """rel-L1 (h, total bed) of float32 vs float64 after ``steps`` SSPRK2 steps."""
+    import torch
+
+    from pyexner_b200 import run_steps
+
+    res = {}
+    for dt in (torch.float32, torch.float64):
+        c, bundle, cfg, mask, st = build_case(n, dt, "cuda")
+        t0 = time.time()
+        run_steps(st, mask, cfg, "SSPRK2", steps, 0.5)
+        torch.cuda.synchronize()
+        res[dt] = (st.to_numpy(), time.time() - t0)
+    a, b = res[torch.float32][0], res[torch.float64][0]
+    s = (slice(1, -1), slice(1, -1))
+
+    def l1(x, y):
+        return float(np.sum(np.abs(x - y)) / np.sum(np.abs(y)))
+
+    return {"steps": steps, "n": n, "h_rel_l1": l1(a["h"][s], b["h"][s]),
+            "bed_rel_l1": l1((a["z"] + a["z_b"])[s], (b["z"] + b["z_b"])[s]),
+            "hu_rel_l1": l1(a["hu"][s], b["hu"][s])}
+
+
+def cpu_oracle_sample(n=256, steps=2):
+    """Float64 NumPy oracle (single thread) on the same generator at n x n."""
+    from oracle import boundaries as OB
+    from oracle import integrators as OI
+    from oracle import roe_exner as ORE
+    from pyexner_b200 import cases
+
+    c = cases.gaussian_bed(n)
+    bcs = OB.Boundaries("Roe Exner", c["params"]["boundaries"], c["X"], c["Y"])
+    st = {k: np.array(v) for k, v in c["arrs"].items()}
+    st["n_b"] = np.zeros_like(st["h"])
+    st["seds"] = c["seds"]
+    mask = OB.roe_exner_mask(st["z"].copy(), bcs.boundary_mask)
+    st = ORE.init(st, mask, bcs, True)
+    OI.run_roe_exner(st, mask, bcs, True, c["dx"], 0.5, 1, "SSPRK2")  # warm-up
+    t0 = time.perf_counter()
+    OI.run_roe_exner(st, mask, bcs, True, c["dx"], 0.5, steps, "SSPRK2")
+    sec = time.perf_counter() - t0
+    return n * n * steps / sec, f"{n}x{n} Gaussian-bed case, {steps} SSPRK2 steps, float64 NumPy oracle"
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    n = 256
+    per = []
+    for _ in range(args.warmup):
+        cpu_oracle_sample(n, 1)
+    for _ in range(args.steps):
+        v, sample = cpu_oracle_sample(n, 1)
+        per.append(v)
+    v = float(np.mean(per))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * n * n / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Gaussian bed)",
+            "config": {"workload": f"roe_exner_gaussian_bed_{n}x{n}_ssprk2 (bounded CPU sample of the 2048x2048 case)"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--n", type=int, default=2048)
+    ap.add_argument("--impl", default="b200")
+    ap.add_argument("--accuracy-steps", type=int, default=2000)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    from pyexner_b200 import build
+
+    if rank == 0:
+        build.build()
+    if world > 1:
+        dist.barrier()
+
+    n = args.n
+    ncell = n * n
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    # ---- float32 device loop (replicas: every rank advances its own copy; no exchange)
+    c, bundle, cfg, mask, st = build_case(n, torch.float32, "cuda")
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        sec, b = timed_device_loop(st, mask, cfg, args.steps, args.warmup, flush)
+    t = torch.tensor([sec], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    sec = float(t)
+    value = world * ncell * args.steps / sec
+    kt = kernel_breakdown(st, b, mask, cfg, max(3, args.steps // 2), flush)
+    hbm, peak_kind = peaks()
+    esz = 4
+    stage_bytes = (WORDS_STAGE1 + WORDS_STAGE2) * esz * ncell
+    stage_time = kt["stage1"] + kt["stage2"]
+    achieved = stage_bytes / stage_time / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "re_stage_f32_gaussian_bed.md")
+    if os.path.exists(prof):
+        for line in open(prof):
+            if line.startswith("traffic_bytes_per_step_2048:"):
+                traffic = float(line.split(":")[1]) / 2
+    # ---- float64 device loop, same config
+    c64, b64, cfg64, mask64, st64 = build_case(n, torch.float64, "cuda")
+    sec64, _ = timed_device_loop(st64, mask64, cfg64, max(3, args.steps // 2), args.warmup, flush)
+    value64 = ncell * max(3, args.steps // 2) / sec64
+    del st64
+    # ---- end to end through the public API with host buffers
+    e2e_sec, h2d, d2h = e2e_run(n, torch.float32, args.steps, args.warmup)
+    e2e_val = ncell * args.steps / e2e_sec
+    acc = accuracy_run(n, args.accuracy_steps) if args.accuracy_steps > 0 else None
+    if rank != 0:
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    cpu = None
+    if not args.no_cpu:
+        v, sample = cpu_oracle_sample(256, 2)
+        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Gaussian bed)",
+        "config": {"workload": f"roe_exner_gaussian_bed_{n}x{n}_mpm_ssprk2_f32", "cells": ncell,
+                   "parallelism": f"replicas{world}", "l2": "256 MiB flush between timed steps (not timed)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": traffic, "peak_kind": peak_kind,
+                     "kernel": "re_stage_kernel (stage 1 + stage 2 of one step)",
+                     "algorithmic_bytes_per_step": stage_bytes,
+                     "ms": {k: 1e3 * v for k, v in kt.items()}},
+        "fp64": {"value": value64, "unit": UNIT, "fp32_over_fp64": value / world / value64},
+        "accuracy": acc,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
+                "d2h_bytes_per_step": d2h / args.steps,
+                "note": "pinned host state -> device, init + K steps via run_steps, final state -> host"},
+        "gpu_launches": 3 * args.steps,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

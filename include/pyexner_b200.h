@@ -1,0 +1,184 @@
+/*
+ * pyexner_b200 — C ABI of the B200 (sm_100a) explicit finite-volume step of PyExner.
+ *
+ * This boundary replaces the jitted JAX calls that PyExner's integrators make on its
+ * solver bundles (PyExner src/PyExner/solvers/registry.py:18-38):
+ *
+ *   step_fn(state, time, dt, mask, config) -> state        roe_exner_solver.py:80-116, roe_solver.py:40-54
+ *   compute_dt_fn(state, cfl, mask, config) -> dt           roe_exner_solver.py:118-122, roe_solver.py:56-60
+ *   init_fn(state, mask, config) -> state                  roe_exner_solver.py:58-78
+ *
+ * and the device loops of the integrators that drive them
+ * (src/PyExner/integrators/forwardeuler.py:37-49, src/PyExner/integrators/SSPRK2.py:30-51).
+ *
+ * Conventions
+ *   - Every plane is a row-major (ny, nx) array INCLUDING the one-cell ring, with a
+ *     row pitch given in elements.  Row index grows toward -y: y-faces carry the normal
+ *     (0,-1) (roe_exner.py:577).  All planes of one call share ny, nx, pitch and dtype.
+ *   - dtype PXB_F32 or PXB_F64 selects the arithmetic of every kernel of a plan.
+ *   - Device pointers are owned by the caller.  A plan allocates its small tables
+ *     (boundary recipes, the CFL reduction word, the error word) once, in
+ *     pxb_*_plan_create; no call after that allocates.
+ *   - Every call is stream-ordered on the given cudaStream_t (may be 0) and returns a
+ *     status code; pxb_last_error() gives the message of the last failure on the
+ *     calling thread.
+ */
+#ifndef PYEXNER_B200_H
+#define PYEXNER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define PXB_OK 0
+#define PXB_ERR_ARG 1        /* bad argument (null pointer, size, dtype, layout)      */
+#define PXB_ERR_CUDA 2       /* a CUDA call failed                                     */
+#define PXB_ERR_NONFINITE 3  /* the device flagged a non-finite dt or state value      */
+#define PXB_ERR_UNSUPPORTED 4/* boundary layout the fused stage kernel does not cover */
+
+#define PXB_F32 0
+#define PXB_F64 1
+
+#define PXB_FE 0     /* Forward Euler, forwardeuler.py:37-49        */
+#define PXB_SSPRK2 1 /* SSPRK2 (intended form), SSPRK2.py:30-51     */
+
+/* Boundary handler kinds (PyExner BOUNDARY_REGISTRY names, "<flux_scheme> <type>"). */
+#define PXB_BC_RE_REFLECTIVE 1       /* "Roe Exner Reflective"      roeexner_reflective.py:17-63      */
+#define PXB_BC_RE_TRANSMISSIVE 2     /* "Roe Exner Transmissive"    roeexner_transmissive.py:17-31    */
+#define PXB_BC_RE_TRANSMISSIVEBED 3  /* "Roe Exner TransmissiveBed" roeexner_transmissivebed.py:17-27 */
+#define PXB_BC_RE_CONSTANTINFLUX 4   /* "Roe Exner ConstantInflux"  roeexner_constantinflux.py:18-48  */
+#define PXB_BC_ROE_REFLECTIVE 5      /* "Roe Reflective"            roe_reflective.py:18-44           */
+#define PXB_BC_ROE_TRANSMISSIVE 6    /* "Roe Transmissive"          roe_transmissive.py:17-43         */
+
+/* One boundary handler: cells by (flat row*pitch+col) index, donors alike.
+ * Replaces a handler object built by BoundaryManager (boundary_registry.py:132-171)
+ * with the index maps of compute_reflective_indices (boundary_registry.py:61-82). */
+typedef struct pxb_bc_handler {
+    int32_t kind;
+    int32_t count;          /* number of (boundary, donor) pairs            */
+    const int64_t* cells;   /* host array, `count` boundary cells           */
+    const int64_t* donors;  /* host array, `count` donor (interior) cells   */
+    double nx, ny;          /* outward normal as given in the YAML          */
+    double hu_const, hv_const; /* ConstantInflux: float32(values[0]*values[1]), float32(values[0]*values[2]) */
+} pxb_bc_handler;
+
+/* Per ring cell, the boundary result after all handlers, as a function of the
+ * pre-boundary values of one donor cell per field group, resolved by the library from
+ * the ordered handlers at plan creation (internal table; listed here because its
+ * layout is part of the device-side contract).  dy/dx are donor offsets in rows/columns.
+ * flags: 1 h, 2 momentum, 4 momentum is constant (m[0], m[1]), 8 z_b, 16 G.
+ * momentum: hu' = m[0]*hu + m[1]*hv, hv' = m[2]*hu + m[3]*hv (donor values).
+ * Table layout: top row [nx], bottom row [nx], left column [ny], right column [ny]. */
+typedef struct pxb_ring_recipe {
+    int8_t h_dy, h_dx, m_dy, m_dx, zb_dy, zb_dx, g_dy, g_dx;
+    uint32_t flags;
+    uint32_t pad;
+    double m[4];
+} pxb_ring_recipe;
+
+/* Roe-Exner state planes (RoeExnerState, src/PyExner/state/roe_exner_state.py:8-48). */
+typedef struct pxb_re_fields {
+    void* h;
+    void* hu;
+    void* hv;
+    void* z;    /* rigid bed (static)                         */
+    void* z_b;  /* erodible layer                              */
+    void* n;    /* Manning (only boundary handlers touch it)   */
+    void* n_b;  /* Manning used in the flux (frozen after init) */
+    void* G;    /* grass factor                                */
+} pxb_re_fields;
+
+/* Plain Roe state planes (RoeState, src/PyExner/state/roe_state.py:8-61). */
+typedef struct pxb_roe_fields {
+    void* h;
+    void* hu;
+    void* hv;
+    void* z;
+    void* n;
+} pxb_roe_fields;
+
+typedef struct pxb_re_plan pxb_re_plan;
+typedef struct pxb_roe_plan pxb_roe_plan;
+
+/* Configuration of a Roe-Exner plan.
+ * mpm = 1: grass factor from Meyer-Peter & Mueller (roe_exner.py:85-130), erosion.grass_factor "MPM";
+ * mpm = 0: constant grass factor read from the state (roe_exner.py:136-140).
+ * seds: host pointer to the 7 x nsed matrix of src/PyExner/io/pnetcdf_reader.py:136-158
+ *       (row-major: fraction, d50, density, k_d, k_e, theta_c, porosity), nsed <= 8.
+ * nodata: device uint8 plane of mask[0] (roe_exner_solver.py:21-39) or NULL if all false. */
+typedef struct pxb_re_config {
+    int32_t ny, nx;
+    int64_t pitch;
+    int32_t dtype;
+    int32_t mpm;
+    double dx;
+    const double* seds;
+    int32_t nsed;
+    const uint8_t* nodata;
+    const pxb_bc_handler* handlers; /* in YAML order; resolved into ring recipes at plan creation */
+    int32_t nhandlers;
+    int32_t band_rows;              /* rows per warp band of the stage kernel; 0 = automatic   */
+} pxb_re_config;
+
+/* --- Roe-Exner ------------------------------------------------------------------ */
+int pxb_re_plan_create(const pxb_re_config* cfg, pxb_re_plan** out);
+int pxb_re_plan_destroy(pxb_re_plan* plan);
+
+/* init_fn_roeexner (roe_exner_solver.py:58-78): n_b, G, then the handlers at t = 0, in place. */
+int pxb_re_init(pxb_re_plan* plan, const pxb_re_fields* f, void* stream);
+
+/* compute_dt_roeexner (roe_exner_solver.py:118-122): dt = max(cfl * min_faces dt_face, 1e-6)
+ * written to dt_dev (one element of the plan dtype, device memory). */
+int pxb_re_cfl(pxb_re_plan* plan, const pxb_re_fields* f, double cfl, void* dt_dev, void* stream);
+
+/* step_fn_roeexner (roe_exner_solver.py:80-116): one stage from `in` to `out` with the
+ * device scalar dt.  If `avg` is not NULL the result is 0.5*avg + 0.5*stage(in) on
+ * h, hu, hv, z_b, G (the SSPRK2 combination, SSPRK2.py:40); out may alias avg, never in.
+ * out->G may be NULL when the caller does not need G (it is recomputed in MPM mode). */
+int pxb_re_stage(pxb_re_plan* plan, const pxb_re_fields* in, const pxb_re_fields* out,
+                 const pxb_re_fields* avg, const void* dt_dev, void* stream);
+
+/* A fixed number of integrator steps (forwardeuler.py:37-49 / SSPRK2.py:30-51 without
+ * output probes).  The state starts and ends in `a`; `b` is scratch state of the same
+ * layout (h, hu, hv, z_b, G are written).  dt_log: device array of nsteps dts or NULL.
+ * The steps are captured once into a CUDA graph and replayed. */
+int pxb_re_run(pxb_re_plan* plan, const pxb_re_fields* a, const pxb_re_fields* b, int32_t nsteps,
+               int32_t scheme, double cfl, void* dt_log, void* stream);
+
+/* Device error word of the plan (non-finite dt or state seen by a kernel): reads it
+ * (synchronising `stream`), clears it, returns PXB_OK or PXB_ERR_NONFINITE. */
+int pxb_re_check(pxb_re_plan* plan, void* stream);
+
+/* --- plain Roe -------------------------------------------------------------------- */
+typedef struct pxb_roe_config {
+    int32_t ny, nx;
+    int64_t pitch;
+    int32_t dtype;
+    double dx;
+    const pxb_bc_handler* handlers;
+    int32_t nhandlers;
+} pxb_roe_config;
+
+int pxb_roe_plan_create(const pxb_roe_config* cfg, pxb_roe_plan** out);
+int pxb_roe_plan_destroy(pxb_roe_plan* plan);
+/* compute_dt_roe (roe_solver.py:56-60, roe.py:13-30): cfl * min over all cells, no floor. */
+int pxb_roe_cfl(pxb_roe_plan* plan, const pxb_roe_fields* f, double cfl, void* dt_dev, void* stream);
+/* step_fn_roe (roe_solver.py:40-54); avg as in pxb_re_stage (h, hu, hv, z, n). */
+int pxb_roe_stage(pxb_roe_plan* plan, const pxb_roe_fields* in, const pxb_roe_fields* out,
+                  const pxb_roe_fields* avg, const void* dt_dev, void* stream);
+int pxb_roe_run(pxb_roe_plan* plan, const pxb_roe_fields* a, const pxb_roe_fields* b, int32_t nsteps,
+                int32_t scheme, double cfl, void* dt_log, void* stream);
+int pxb_roe_check(pxb_roe_plan* plan, void* stream);
+
+/* --- misc ------------------------------------------------------------------------- */
+const char* pxb_last_error(void);
+int pxb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PYEXNER_B200_H */

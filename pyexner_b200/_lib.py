@@ -1,0 +1,141 @@
+"""ctypes binding of ``libpyexner_b200.so`` (the C ABI in include/pyexner_b200.h).
+
+There is no fallback: if the library is missing or a CUDA device is absent the calls
+raise.  The product path never computes on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+from ctypes import POINTER, c_double, c_int, c_int32, c_int64, c_void_p
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpyexner_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "pyexner_b200.h")
+
+OK, ERR_ARG, ERR_CUDA, ERR_NONFINITE, ERR_UNSUPPORTED = 0, 1, 2, 3, 4
+F32, F64 = 0, 1
+FE, SSPRK2 = 0, 1
+BC_KINDS = {
+    "Roe Exner Reflective": 1,
+    "Roe Exner Transmissive": 2,
+    "Roe Exner TransmissiveBed": 3,
+    "Roe Exner ConstantInflux": 4,
+    "Roe Reflective": 5,
+    "Roe Transmissive": 6,
+}
+
+
+class BcHandler(ctypes.Structure):
+    _fields_ = [
+        ("kind", c_int32),
+        ("count", c_int32),
+        ("cells", c_void_p),
+        ("donors", c_void_p),
+        ("nx", c_double),
+        ("ny", c_double),
+        ("hu_const", c_double),
+        ("hv_const", c_double),
+    ]
+
+
+class REFields(ctypes.Structure):
+    _fields_ = [(n, c_void_p) for n in ("h", "hu", "hv", "z", "z_b", "n", "n_b", "G")]
+
+
+class RoeFields(ctypes.Structure):
+    _fields_ = [(n, c_void_p) for n in ("h", "hu", "hv", "z", "n")]
+
+
+class REConfig(ctypes.Structure):
+    _fields_ = [
+        ("ny", c_int32),
+        ("nx", c_int32),
+        ("pitch", c_int64),
+        ("dtype", c_int32),
+        ("mpm", c_int32),
+        ("dx", c_double),
+        ("seds", c_void_p),
+        ("nsed", c_int32),
+        ("nodata", c_void_p),
+        ("handlers", POINTER(BcHandler)),
+        ("nhandlers", c_int32),
+        ("band_rows", c_int32),
+    ]
+
+
+class RoeConfig(ctypes.Structure):
+    _fields_ = [
+        ("ny", c_int32),
+        ("nx", c_int32),
+        ("pitch", c_int64),
+        ("dtype", c_int32),
+        ("dx", c_double),
+        ("handlers", POINTER(BcHandler)),
+        ("nhandlers", c_int32),
+    ]
+
+
+class PxbError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"pyexner_b200 error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+# (name, argtypes) of every entry point declared in include/pyexner_b200.h
+SIGNATURES = {
+    "pxb_re_plan_create": [POINTER(REConfig), POINTER(c_void_p)],
+    "pxb_re_plan_destroy": [c_void_p],
+    "pxb_re_init": [c_void_p, POINTER(REFields), c_void_p],
+    "pxb_re_cfl": [c_void_p, POINTER(REFields), c_double, c_void_p, c_void_p],
+    "pxb_re_stage": [c_void_p, POINTER(REFields), POINTER(REFields), POINTER(REFields), c_void_p, c_void_p],
+    "pxb_re_run": [c_void_p, POINTER(REFields), POINTER(REFields), c_int32, c_int32, c_double, c_void_p, c_void_p],
+    "pxb_re_check": [c_void_p, c_void_p],
+    "pxb_roe_plan_create": [POINTER(RoeConfig), POINTER(c_void_p)],
+    "pxb_roe_plan_destroy": [c_void_p],
+    "pxb_roe_cfl": [c_void_p, POINTER(RoeFields), c_double, c_void_p, c_void_p],
+    "pxb_roe_stage": [c_void_p, POINTER(RoeFields), POINTER(RoeFields), POINTER(RoeFields), c_void_p, c_void_p],
+    "pxb_roe_run": [c_void_p, POINTER(RoeFields), POINTER(RoeFields), c_int32, c_int32, c_double, c_void_p, c_void_p],
+    "pxb_roe_check": [c_void_p, c_void_p],
+    "pxb_version": [],
+}
+
+
+def header_symbols():
+    """Names of the functions declared in include/pyexner_b200.h."""
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(pxb_\w+)\s*\(", txt, re.M)))
+
+
+def load():
+    """Load the library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build it with `python -m pyexner_b200.build` "
+            "(the CUDA path is the only implementation)"
+        )
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, args in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = c_int
+    lib.pxb_last_error.restype = ctypes.c_char_p
+    lib.pxb_last_error.argtypes = []
+    _lib = lib
+    return lib
+
+
+def check(code):
+    if code != OK:
+        msg = load().pxb_last_error().decode(errors="replace")
+        raise PxbError(code, msg)
+
+
+def call(name, *args):
+    check(getattr(load(), name)(*args))

@@ -1,0 +1,76 @@
+"""Build the in-tree CUDA library ``libpyexner_b200.so`` for sm_100a.
+
+    python -m pyexner_b200.build
+
+Three translation units: the float32 kernels, the float64 kernels (with
+``--fmad=false`` so every product and sum rounds on its own, as in the reference's
+float64 arithmetic) and the C ABI.  Objects go to ``pyexner_b200/_build``.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libpyexner_b200.so")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2"]
+
+UNITS = [
+    ("kernels_f32.cu", []),
+    ("kernels_f64.cu", ["-fmad=false"]),
+    ("capi.cu", []),
+]
+
+
+def nvcc():
+    exe = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(exe):
+        raise RuntimeError("nvcc not found; the CUDA toolkit is required to build pyexner_b200")
+    return exe
+
+
+def sources():
+    out = []
+    for name in os.listdir(CSRC):
+        if name.endswith((".cu", ".cuh", ".h")):
+            out.append(os.path.join(CSRC, name))
+    out.append(os.path.join(os.path.dirname(HERE), "include", "pyexner_b200.h"))
+    return out
+
+
+def up_to_date():
+    if not os.path.exists(LIB):
+        return False
+    t = os.path.getmtime(LIB)
+    return all(os.path.getmtime(s) <= t for s in sources())
+
+
+def build(force=False, verbose=False):
+    if not force and up_to_date():
+        return LIB
+    os.makedirs(BUILD, exist_ok=True)
+    objs = []
+    for src, extra in UNITS:
+        obj = os.path.join(BUILD, src.replace(".cu", ".o"))
+        cmd = [nvcc(), *ARCH, *COMMON, *extra, "-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        objs.append(obj)
+    tmp = LIB + ".tmp"
+    cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

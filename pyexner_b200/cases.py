@@ -1,0 +1,99 @@
+"""Seeded synthetic workloads (no dataset is involved; every input is generated).
+
+* ``dambreak_roe``   plain Roe dam-break on the unit square: 256 x 256 cells
+  (+ ring), dx = 1/256, h = 1 for x < 0.5 else 0.1, at rest, flat bed, Roe Reflective
+  walls on the four sides (left, right, bottom, top), CFL 0.5, SSPRK2, 200 steps, float64.
+* ``gaussian_bed``   Roe-Exner on an N x N grid (+ ring), dx = 0.01 m.  Total bed
+  z_t = 0.05 * sum_{k<16} A_k exp(-|x - c_k|^2 / (2 s_k^2)) with c_k ~ U(domain),
+  s_k ~ U(0.05, 0.3) L, A_k ~ U(-1, 1) (seed ``seed_bed``); rigid bed z = min(z_t) - 0.05
+  (constant), erodible layer z_b = z_t - z; h = max(0, (0.3 - z_t) (1 + 0.02 U(-1, 1)))
+  (seed ``seed_noise``), hu = 0.1 h, hv = 0, n = 0; MPM with one sediment
+  (d = 1.61e-3 m, 2630 kg/m^3, porosity 0.42); Transmissive + TransmissiveBed in x,
+  Reflective in y applied last (they win the corners).  N = 2048 is the 2000-step
+  accuracy/throughput case, N = 8192 the 500-step bandwidth case.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .boundaries import BoundaryManager, index_coords, ring_boundaries
+
+SED_ONE = {"s1": dict(fraction=1.0, diameter=1.61e-3, density=2630.0, deposition_flux=0.0, erosion_flux=0.0)}
+
+
+def seds_matrix(erosion):
+    """7 x nsed matrix of src/PyExner/io/pnetcdf_reader.py:136-162 (theta_c = 0.047)."""
+    grass = erosion["grass_factor"]
+    if not isinstance(grass, str):
+        return np.zeros((1, 1))
+    rows = []
+    for key in erosion["sediments"]:
+        s = erosion["sediments"][key]
+        rows.append([s["fraction"], s["diameter"], s["density"], s["deposition_flux"], s["erosion_flux"], 0.047,
+                     erosion["bulk_porosity"]])
+    return np.array(rows, dtype=np.float64).T
+
+
+def dambreak_roe(n=256):
+    ny = nx = n + 2
+    dx = 1.0 / n
+    xc = (np.arange(nx) - 0.5) * dx
+    h = np.where(xc[None, :] < 0.5, 1.0, 0.1) * np.ones((ny, nx))
+    z = np.zeros((ny, nx))
+    arrs = dict(h=h, hu=np.zeros_like(h), hv=np.zeros_like(h), z=z, n=np.zeros_like(h))
+    bspec = ring_boundaries(ny, nx, ["Reflective"], ["Reflective"], ["Reflective"], ["Reflective"])
+    X, Y = index_coords(ny, nx)
+    params = dict(flux_scheme="Roe", boundaries=bspec, cfl=0.5, integrator="SSPRK2")
+    return dict(arrs=arrs, dx=dx, params=params, boundaries=BoundaryManager(params, X, Y), X=X, Y=Y)
+
+
+def gaussian_bed_fields(n, dx=0.01, seed_bed=1, seed_noise=2, device=None):
+    """Planes of the Gaussian-bed case as float64 numpy arrays (ring included).
+
+    With ``device`` set (e.g. "cuda") the bed sum is evaluated with torch on that device,
+    which is what makes the 8192^2 case quick to build; the numbers are the same
+    float64 expression either way."""
+    ny = nx = n + 2
+    L = n * dx
+    rb = np.random.default_rng(seed_bed)
+    ck = rb.uniform(0.0, L, (16, 2))
+    sk = rb.uniform(0.05, 0.3, 16) * L
+    ak = rb.uniform(-1.0, 1.0, 16)
+    xc = (np.arange(nx) - 0.5) * dx
+    yc = (ny - 1 - np.arange(ny) - 0.5) * dx
+    if device is None:
+        zt = np.zeros((ny, nx))
+        for k in range(16):
+            gx = np.exp(-((xc - ck[k, 0]) ** 2) / (2 * sk[k] ** 2))
+            gy = np.exp(-((yc - ck[k, 1]) ** 2) / (2 * sk[k] ** 2))
+            zt += ak[k] * np.outer(gy, gx)
+        zt *= 0.05
+    else:
+        import torch
+
+        tx = torch.tensor(xc, dtype=torch.float64, device=device)
+        ty = torch.tensor(yc, dtype=torch.float64, device=device)
+        acc = torch.zeros((ny, nx), dtype=torch.float64, device=device)
+        for k in range(16):
+            gx = torch.exp(-((tx - ck[k, 0]) ** 2) / (2 * sk[k] ** 2))
+            gy = torch.exp(-((ty - ck[k, 1]) ** 2) / (2 * sk[k] ** 2))
+            acc += ak[k] * torch.outer(gy, gx)
+        zt = (0.05 * acc).cpu().numpy()
+    z = np.full((ny, nx), zt.min() - 0.05)
+    zb = zt - z
+    rn = np.random.default_rng(seed_noise)
+    noise = rn.uniform(-1.0, 1.0, (ny, nx))
+    h = np.maximum(0.0, (0.3 - zt) * (1.0 + 0.02 * noise))
+    return dict(h=h, hu=0.1 * h, hv=np.zeros_like(h), z=z, z_b=zb, n=np.zeros_like(h), G=np.zeros_like(h))
+
+
+def gaussian_bed(n, dx=0.01, seed_bed=1, seed_noise=2, device=None):
+    ny = nx = n + 2
+    arrs = gaussian_bed_fields(n, dx, seed_bed, seed_noise, device)
+    erosion = dict(grass_factor="MPM", bulk_porosity=0.42, sediments=SED_ONE)
+    bspec = ring_boundaries(ny, nx, ["Transmissive", "TransmissiveBed"], ["Transmissive", "TransmissiveBed"],
+                            ["Reflective"], ["Reflective"])
+    X, Y = index_coords(ny, nx)
+    params = dict(flux_scheme="Roe Exner", integrator="SSPRK2", cfl=0.5, erosion=erosion, boundaries=bspec)
+    return dict(arrs=arrs, seds=seds_matrix(erosion), dx=dx, params=params,
+                boundaries=BoundaryManager(params, X, Y), X=X, Y=Y)

@@ -1,0 +1,901 @@
+// extern "C" boundary of the library (declared in include/pyexner_b200.h).
+//
+// Host-side responsibilities:
+//   * validate arguments and layouts, and report errors through status codes plus a
+//     thread-local message;
+//   * resolve the ordered boundary handlers into per-ring-cell recipes (the symbolic
+//     equivalent of applying PyExner's handlers one after another,
+//     src/PyExner/domain/boundary_registry.py:183-187) and upload them once;
+//   * turn the sediment matrix into per-class constants;
+//   * size the warp strips / row bands of the stage and CFL kernels to the device;
+//   * capture the fixed-step integrator loops into CUDA graphs and replay them.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "pxb_launch.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define PXB_CUDA(call)                                                                              \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess) return fail(PXB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// ------------------------------------------------------------------ recipe resolution
+// Expression of one field group of one cell after some handlers: the value of that
+// group at cell `src` before the whole application, mapped by `m` (momentum only),
+// or a constant pair (momentum of ConstantInflux).
+struct GroupExpr {
+    long long src = -1;  // -1: identity (the cell itself)
+    bool is_const = false;
+    double m[4] = {1, 0, 0, 1};
+    bool set = false;
+};
+struct CellExpr {
+    GroupExpr h, mom, zb, g, n, z;
+};
+
+struct Resolved {
+    std::vector<pxb_ring_recipe> ring;  // 2*nx + 2*ny
+    std::string error;
+};
+
+GroupExpr ident(long long cell) {
+    GroupExpr e;
+    e.src = cell;
+    return e;
+}
+
+GroupExpr get(const std::unordered_map<long long, CellExpr>& mp, long long cell, GroupExpr CellExpr::*grp) {
+    auto it = mp.find(cell);
+    if (it == mp.end() || !((it->second).*grp).set) return ident(cell);
+    return (it->second).*grp;
+}
+
+GroupExpr map_mom(const GroupExpr& e, const double a[4]) {
+    GroupExpr o = e;
+    if (e.is_const) {
+        o.m[0] = a[0] * e.m[0] + a[1] * e.m[1];
+        o.m[1] = a[2] * e.m[0] + a[3] * e.m[1];
+        o.m[2] = o.m[3] = 0;
+    } else {
+        o.m[0] = a[0] * e.m[0] + a[1] * e.m[2];
+        o.m[1] = a[0] * e.m[1] + a[1] * e.m[3];
+        o.m[2] = a[2] * e.m[0] + a[3] * e.m[2];
+        o.m[3] = a[2] * e.m[1] + a[3] * e.m[3];
+    }
+    return o;
+}
+
+bool is_ring(long long r, long long c, long long ny, long long nx) {
+    return r == 0 || r == ny - 1 || c == 0 || c == nx - 1;
+}
+
+// Apply the handler sequence symbolically; flat cell ids are row*nx + col.
+Resolved resolve(const pxb_bc_handler* hs, int nh, int ny, int nx, long long pitch, bool roe, bool need_idempotent) {
+    Resolved R;
+    std::unordered_map<long long, CellExpr> mp;
+    for (int k = 0; k < nh; ++k) {
+        const pxb_bc_handler& H = hs[k];
+        std::vector<std::pair<long long, CellExpr>> upd;
+        upd.reserve(H.count);
+        for (int p = 0; p < H.count; ++p) {
+            const long long bc = H.cells[p], dc = H.donors[p];
+            const long long b = (bc / pitch) * nx + (bc % pitch);
+            const long long d = (dc / pitch) * nx + (dc % pitch);
+            auto it = mp.find(b);
+            CellExpr ne = (it == mp.end()) ? CellExpr() : it->second;
+            auto setg = [](GroupExpr& dst, GroupExpr v) { v.set = true; dst = v; };
+            const double nxv = H.nx, nyv = H.ny;
+            switch (H.kind) {
+                case PXB_BC_RE_REFLECTIVE: {
+                    const double a[4] = {nyv * nyv - nxv * nxv, -2 * nxv * nyv, -2 * nxv * nyv, nxv * nxv - nyv * nyv};
+                    setg(ne.h, get(mp, d, &CellExpr::h));
+                    setg(ne.zb, get(mp, d, &CellExpr::zb));
+                    setg(ne.n, get(mp, d, &CellExpr::n));
+                    setg(ne.g, get(mp, d, &CellExpr::g));
+                    setg(ne.mom, map_mom(get(mp, d, &CellExpr::mom), a));
+                    break;
+                }
+                case PXB_BC_RE_TRANSMISSIVE:
+                    setg(ne.h, get(mp, d, &CellExpr::h));
+                    setg(ne.mom, get(mp, d, &CellExpr::mom));
+                    break;
+                case PXB_BC_RE_TRANSMISSIVEBED:
+                    setg(ne.zb, get(mp, d, &CellExpr::zb));
+                    break;
+                case PXB_BC_RE_CONSTANTINFLUX: {
+                    GroupExpr e;
+                    e.is_const = true;
+                    e.m[0] = H.hu_const;
+                    e.m[1] = H.hv_const;
+                    e.m[2] = e.m[3] = 0;
+                    setg(ne.mom, e);
+                    break;
+                }
+                case PXB_BC_ROE_REFLECTIVE: {
+                    const double a[4] = {1 - 2 * nxv * nxv, 0, 0, 1 - 2 * nyv * nyv};
+                    setg(ne.h, get(mp, d, &CellExpr::h));
+                    setg(ne.z, get(mp, d, &CellExpr::z));
+                    setg(ne.n, get(mp, d, &CellExpr::n));
+                    setg(ne.mom, map_mom(get(mp, d, &CellExpr::mom), a));
+                    break;
+                }
+                case PXB_BC_ROE_TRANSMISSIVE:
+                    setg(ne.h, get(mp, d, &CellExpr::h));
+                    setg(ne.z, get(mp, d, &CellExpr::z));
+                    setg(ne.n, get(mp, d, &CellExpr::n));
+                    setg(ne.mom, get(mp, d, &CellExpr::mom));
+                    break;
+                default:
+                    R.error = "unknown boundary kind " + std::to_string(H.kind);
+                    return R;
+            }
+            upd.emplace_back(b, ne);
+        }
+        for (auto& u : upd) mp[u.first] = u.second;  // scatter after the gather
+    }
+    R.ring.assign((size_t)(2 * nx + 2 * ny), pxb_ring_recipe{});
+    for (auto& kv : mp) {
+        const long long cell = kv.first;
+        const long long r = cell / nx, c = cell % nx;
+        if (!is_ring(r, c, ny, nx)) {
+            R.error = "boundary cell (" + std::to_string(r) + "," + std::to_string(c) +
+                      ") is off the outer ring; the stage kernels support ring boundaries only";
+            return R;
+        }
+        const CellExpr& e = kv.second;
+        pxb_ring_recipe rc{};
+        auto off = [&](const GroupExpr& g, int8_t& dy, int8_t& dx) -> bool {
+            if (!g.set || g.is_const) return true;
+            const long long sr = g.src / nx, sc = g.src % nx;
+            const long long oy = sr - r, ox = sc - c;
+            if (oy < -1 || oy > 1 || ox < -1 || ox > 1) return false;
+            if (oy != 0 && !((r == 0 && oy > 0) || (r == ny - 1 && oy < 0))) return false;
+            if (ox != 0 && !((c == 0 && ox > 0) || (c == nx - 1 && ox < 0))) return false;
+            dy = (int8_t)oy;
+            dx = (int8_t)ox;
+            return true;
+        };
+        bool ok = off(e.h, rc.h_dy, rc.h_dx) && off(e.mom, rc.m_dy, rc.m_dx) && off(e.zb, rc.zb_dy, rc.zb_dx) &&
+                  off(e.g, rc.g_dy, rc.g_dx);
+        if (roe && ok) {
+            // Roe handlers write h, z and n together: their donors coincide.
+            if (e.z.set && e.z.src != e.h.src) ok = false;
+            if (e.n.set && e.n.src != e.h.src) ok = false;
+        }
+        if (!ok) {
+            R.error = "boundary cell (" + std::to_string(r) + "," + std::to_string(c) +
+                      ") takes its value from a cell the stage kernels cannot reach (donor must be an adjacent cell "
+                      "toward the interior)";
+            return R;
+        }
+        if (e.h.set) rc.flags |= 1u;
+        if (e.mom.set) {
+            rc.flags |= 2u;
+            if (e.mom.is_const) rc.flags |= 4u;
+            for (int q = 0; q < 4; ++q) rc.m[q] = e.mom.m[q];
+        }
+        if (e.zb.set) rc.flags |= 8u;
+        if (e.g.set) rc.flags |= 16u;
+        if (r == 0) R.ring[(size_t)c] = rc;
+        if (r == ny - 1) R.ring[(size_t)(nx + c)] = rc;
+        if (c == 0) R.ring[(size_t)(2 * nx + r)] = rc;
+        if (c == nx - 1) R.ring[(size_t)(2 * nx + ny + r)] = rc;
+    }
+    if (need_idempotent) {
+        // The Roe-Exner stage stores h, hu, hv after the first application; that is
+        // exact when a second application would not change them, i.e. when no donor
+        // of a hydro recipe carries a hydro recipe itself.
+        for (auto& kv : mp) {
+            const long long cell = kv.first;
+            const CellExpr& e = kv.second;
+            auto bad = [&](const GroupExpr& g, GroupExpr CellExpr::*grp) {
+                if (!g.set || g.is_const) return false;
+                if (g.src == cell) {
+                    if (grp == &CellExpr::mom) return !(g.m[0] == 1 && g.m[1] == 0 && g.m[2] == 0 && g.m[3] == 1);
+                    return false;
+                }
+                auto it = mp.find(g.src);
+                return it != mp.end() && ((it->second).*grp).set;
+            };
+            if (bad(e.h, &CellExpr::h) || bad(e.mom, &CellExpr::mom)) {
+                const long long r = cell / nx, c = cell % nx;
+                R.error = "boundary cell (" + std::to_string(r) + "," + std::to_string(c) +
+                          ") copies a depth or momentum that is itself a boundary value; a second application would "
+                          "change it";
+                return R;
+            }
+        }
+    }
+    return R;
+}
+
+// ------------------------------------------------------------------ shared plan bits
+struct DevHandler {
+    int kind = 0, count = 0;
+    long long* cells = nullptr;
+    long long* donors = nullptr;
+    double nx = 0, ny = 0, c0 = 0, c1 = 0;
+};
+
+struct Geometry {
+    int band_rows = 0, nstrips = 0, nbands = 0, grid = 0;
+};
+
+Geometry stage_geometry(int ny, int nx, int resident_warps, int want_rows) {
+    Geometry g;
+    g.nstrips = std::max(1, (nx - 3 + PXB_STRIP_OUT - 1) / PXB_STRIP_OUT);
+    int rows = want_rows;
+    if (rows <= 0) {
+        const int target_bands = std::max(1, resident_warps / g.nstrips);
+        rows = std::max(8, (ny - 1 + target_bands - 1) / target_bands);
+    }
+    g.band_rows = rows;
+    g.nbands = std::max(1, (ny - 1 + rows - 1) / rows);
+    const int items = g.nstrips * g.nbands;
+    g.grid = std::max(1, (items + 3) / 4);
+    return g;
+}
+
+Geometry cfl_geometry(int ny, int nx, int resident_warps) {
+    Geometry g;
+    g.nstrips = std::max(1, (nx + 30) / 31);
+    const int target_bands = std::max(1, resident_warps / g.nstrips);
+    g.band_rows = std::max(8, (ny + target_bands - 1) / target_bands);
+    g.nbands = std::max(1, (ny + g.band_rows - 1) / g.band_rows);
+    const int items = g.nstrips * g.nbands;
+    g.grid = std::max(1, (items + 7) / 8);
+    return g;
+}
+
+int upload_handlers(const pxb_bc_handler* hs, int nh, long long max_index, std::vector<DevHandler>& out,
+                    int& maxcount) {
+    maxcount = 0;
+    for (int k = 0; k < nh; ++k) {
+        const pxb_bc_handler& H = hs[k];
+        if (H.count < 0 || (H.count > 0 && (!H.cells || !H.donors)))
+            return fail(PXB_ERR_ARG, "boundary handler " + std::to_string(k) + " has no index arrays");
+        for (int p = 0; p < H.count; ++p)
+            if (H.cells[p] < 0 || H.cells[p] >= max_index || H.donors[p] < 0 || H.donors[p] >= max_index)
+                return fail(PXB_ERR_ARG, "boundary handler " + std::to_string(k) + " indexes outside the grid");
+        DevHandler d;
+        d.kind = H.kind;
+        d.count = H.count;
+        d.nx = H.nx;
+        d.ny = H.ny;
+        d.c0 = H.hu_const;
+        d.c1 = H.hv_const;
+        if (H.count > 0) {
+            PXB_CUDA(cudaMalloc(&d.cells, sizeof(long long) * H.count));
+            PXB_CUDA(cudaMalloc(&d.donors, sizeof(long long) * H.count));
+            PXB_CUDA(cudaMemcpy(d.cells, H.cells, sizeof(long long) * H.count, cudaMemcpyHostToDevice));
+            PXB_CUDA(cudaMemcpy(d.donors, H.donors, sizeof(long long) * H.count, cudaMemcpyHostToDevice));
+        }
+        maxcount = std::max(maxcount, H.count);
+        out.push_back(d);
+    }
+    return PXB_OK;
+}
+
+template <class T>
+void fill_sed(pxb::SedTable<T>& S, const double* seds, int nsed) {
+    std::memset(&S, 0, sizeof(S));
+    S.n = nsed;
+    double por_sum = 0, d50f_sum = 0;
+    for (int k = 0; k < nsed; ++k) {
+        const double frac = seds[0 * nsed + k], d50 = seds[1 * nsed + k], dens = seds[2 * nsed + k];
+        const double thc = seds[5 * nsed + k], por = seds[6 * nsed + k];
+        const double s = dens / 1000.0;
+        const double np_ = std::pow(d50, 1.0 / 6.0) / 21.1;
+        S.s[k].np2 = (T)(np_ * np_);
+        S.s[k].sm1d = (T)((s - 1.0) * d50);
+        S.s[k].thc = (T)thc;
+        S.s[k].np3sg = (T)(std::pow(np_, 3.0) * std::sqrt(9.81));
+        S.s[k].sm1 = (T)(s - 1.0);
+        S.s[k].frac = (T)frac;
+        por_sum += por;
+        d50f_sum += d50 * frac;
+    }
+    S.one_minus_por = (T)(1.0 - por_sum / nsed);
+    S.n_p_mix = (T)(std::pow(d50f_sum / nsed, 1.0 / 6.0) / 21.1);
+}
+
+struct PlanCommon {
+    int ny = 0, nx = 0;
+    long long pitch = 0;
+    int dtype = 0;
+    double dx = 0;
+    int sm_count = 0;
+    std::vector<DevHandler> handlers;
+    pxb_ring_recipe* ring = nullptr;
+    void* bc_tmp = nullptr;
+    pxb::CflScratch* scr = nullptr;
+    void* dt_dev = nullptr;
+    cudaStream_t cap = nullptr;
+    Geometry cfl;
+    // graph cache
+    struct Cached {
+        std::vector<const void*> key;
+        cudaGraphExec_t exec = nullptr;
+    };
+    std::vector<Cached> graphs;
+
+    size_t esize() const { return dtype == PXB_F64 ? 8 : 4; }
+
+    void release() {
+        for (auto& h : handlers) {
+            cudaFree(h.cells);
+            cudaFree(h.donors);
+        }
+        handlers.clear();
+        for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
+        graphs.clear();
+        cudaFree(ring);
+        cudaFree(bc_tmp);
+        cudaFree(scr);
+        cudaFree(dt_dev);
+        if (cap) cudaStreamDestroy(cap);
+        ring = nullptr;
+        bc_tmp = nullptr;
+        scr = nullptr;
+        dt_dev = nullptr;
+        cap = nullptr;
+    }
+};
+
+int common_setup(PlanCommon& P, int ny, int nx, long long pitch, int dtype, double dx, const pxb_bc_handler* hs,
+                 int nh, bool roe) {
+    if (ny < 3 || nx < 3) return fail(PXB_ERR_ARG, "grid must be at least 3 x 3 cells including the ring");
+    if (pitch < nx) return fail(PXB_ERR_ARG, "pitch smaller than nx");
+    if (dtype != PXB_F32 && dtype != PXB_F64) return fail(PXB_ERR_ARG, "dtype must be PXB_F32 or PXB_F64");
+    if (!(dx > 0) || !std::isfinite(dx)) return fail(PXB_ERR_ARG, "dx must be positive and finite");
+    if (nh < 0 || (nh > 0 && !hs)) return fail(PXB_ERR_ARG, "handlers pointer is null");
+    P.ny = ny;
+    P.nx = nx;
+    P.pitch = pitch;
+    P.dtype = dtype;
+    P.dx = dx;
+    int dev = 0;
+    PXB_CUDA(cudaGetDevice(&dev));
+    PXB_CUDA(cudaDeviceGetAttribute(&P.sm_count, cudaDevAttrMultiProcessorCount, dev));
+    if (nh > 0) {
+        Resolved R = resolve(hs, nh, ny, nx, pitch, roe, !roe);
+        if (!R.error.empty()) return fail(PXB_ERR_UNSUPPORTED, R.error);
+        int maxcount = 0;
+        int st = upload_handlers(hs, nh, (long long)(ny - 1) * pitch + nx, P.handlers, maxcount);
+        if (st != PXB_OK) return st;
+        PXB_CUDA(cudaMalloc(&P.ring, sizeof(pxb_ring_recipe) * R.ring.size()));
+        PXB_CUDA(cudaMemcpy(P.ring, R.ring.data(), sizeof(pxb_ring_recipe) * R.ring.size(), cudaMemcpyHostToDevice));
+        PXB_CUDA(cudaMalloc(&P.bc_tmp, 6 * (size_t)std::max(1, maxcount) * P.esize()));
+    }
+    PXB_CUDA(cudaMalloc(&P.scr, sizeof(pxb::CflScratch)));
+    PXB_CUDA(cudaMemset(P.scr, 0, sizeof(pxb::CflScratch)));
+    PXB_CUDA(cudaMalloc(&P.dt_dev, 8));
+    PXB_CUDA(cudaMemset(P.dt_dev, 0, 8));
+    PXB_CUDA(cudaStreamCreateWithFlags(&P.cap, cudaStreamNonBlocking));
+    return PXB_OK;
+}
+
+int check_plan_error(PlanCommon& P, cudaStream_t s) {
+    pxb::CflScratch h{};
+    PXB_CUDA(cudaMemcpyAsync(&h, P.scr, sizeof(h), cudaMemcpyDeviceToHost, s));
+    PXB_CUDA(cudaStreamSynchronize(s));
+    if (h.err != 0) {
+        PXB_CUDA(cudaMemsetAsync(&P.scr->err, 0, sizeof(int), s));
+        PXB_CUDA(cudaStreamSynchronize(s));
+        return fail(PXB_ERR_NONFINITE, (h.err & 2) ? "non-finite time step (dry domain or NaN state)"
+                                                   : "non-finite value in the updated state");
+    }
+    return PXB_OK;
+}
+
+// Run `body` captured into a graph (cached per key) and launch it `reps` times on `s`.
+template <class F>
+int run_graph(PlanCommon& P, const std::vector<const void*>& key, int reps, cudaStream_t s, F body) {
+    cudaGraphExec_t exec = nullptr;
+    for (auto& g : P.graphs)
+        if (g.key == key) exec = g.exec;
+    if (!exec) {
+        cudaGraph_t graph;
+        PXB_CUDA(cudaStreamBeginCapture(P.cap, cudaStreamCaptureModeThreadLocal));
+        const int st = body(P.cap);
+        cudaGraph_t tmp = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(P.cap, &tmp);
+        if (st != PXB_OK) {
+            if (tmp) cudaGraphDestroy(tmp);
+            return st;
+        }
+        if (ec != cudaSuccess) return fail(PXB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
+        graph = tmp;
+        PXB_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+        cudaGraphDestroy(graph);
+        PlanCommon::Cached c;
+        c.key = key;
+        c.exec = exec;
+        P.graphs.push_back(c);
+    }
+    for (int i = 0; i < reps; ++i) PXB_CUDA(cudaGraphLaunch(exec, s));
+    return PXB_OK;
+}
+
+}  // namespace
+
+// =====================================================================================
+struct pxb_re_plan {
+    PlanCommon c;
+    int mpm = 0;
+    const uint8_t* nodata = nullptr;
+    Geometry stage[8];  // by (mpm, mask, avg) variant: band geometry from its occupancy
+    int want_rows = 0;
+    pxb::SedTable<float> sedf;
+    pxb::SedTable<double> sedd;
+};
+
+struct pxb_roe_plan {
+    PlanCommon c;
+};
+
+namespace {
+
+template <class T>
+const pxb::SedTable<T>& sed_of(const pxb_re_plan* p);
+template <>
+const pxb::SedTable<float>& sed_of<float>(const pxb_re_plan* p) { return p->sedf; }
+template <>
+const pxb::SedTable<double>& sed_of<double>(const pxb_re_plan* p) { return p->sedd; }
+
+int check_fields(const pxb_re_fields* f, bool need_g) {
+    if (!f) return fail(PXB_ERR_ARG, "fields pointer is null");
+    if (!f->h || !f->hu || !f->hv || !f->z_b) return fail(PXB_ERR_ARG, "h, hu, hv and z_b must be set");
+    if (need_g && !f->G) return fail(PXB_ERR_ARG, "G must be set");
+    return PXB_OK;
+}
+
+template <class T>
+int re_cfl_impl(pxb_re_plan* P, const pxb_re_fields* f, double cfl, void* dt_out, void* dt_log, cudaStream_t s) {
+    pxb::CflArgs<T> a{};
+    a.ny = P->c.ny;
+    a.nx = P->c.nx;
+    a.pitch = P->c.pitch;
+    a.h = (const T*)f->h;
+    a.hu = (const T*)f->hu;
+    a.hv = (const T*)f->hv;
+    a.G = (const T*)f->G;
+    a.nodata = P->nodata;
+    a.dx = (T)P->c.dx;
+    a.cfl = (T)cfl;
+    a.floor_dt = (T)pxb::DT_FLOOR;
+    a.scr = P->c.scr;
+    a.dt_out = (T*)dt_out;
+    a.dt_log = (T*)dt_log;
+    a.band_rows = P->c.cfl.band_rows;
+    a.nstrips = P->c.cfl.nstrips;
+    a.nbands = P->c.cfl.nbands;
+    PXB_CUDA(pxb::launch_re_cfl<T>(a, P->nodata != nullptr, P->c.cfl.grid, s));
+    return PXB_OK;
+}
+
+template <class T>
+int re_stage_impl(pxb_re_plan* P, const pxb_re_fields* in, const pxb_re_fields* out, const pxb_re_fields* avg,
+                  const void* dt, cudaStream_t s) {
+    pxb::REStageArgs<T> a{};
+    a.ny = P->c.ny;
+    a.nx = P->c.nx;
+    a.pitch = P->c.pitch;
+    a.dx = (T)P->c.dx;
+    a.h = (const T*)in->h;
+    a.hu = (const T*)in->hu;
+    a.hv = (const T*)in->hv;
+    a.zb = (const T*)in->z_b;
+    a.z = (const T*)in->z;
+    a.nb = (const T*)in->n_b;
+    a.G = (const T*)in->G;
+    a.nodata = P->nodata;
+    a.oh = (T*)out->h;
+    a.ohu = (T*)out->hu;
+    a.ohv = (T*)out->hv;
+    a.ozb = (T*)out->z_b;
+    a.oG = (T*)out->G;
+    if (avg) {
+        a.ah = (const T*)avg->h;
+        a.ahu = (const T*)avg->hu;
+        a.ahv = (const T*)avg->hv;
+        a.azb = (const T*)avg->z_b;
+        a.aG = (const T*)avg->G;
+    }
+    a.dt = (const T*)dt;
+    a.ring = P->c.ring;
+    a.sed = sed_of<T>(P);
+    const int v = (P->mpm ? 4 : 0) | (P->nodata ? 2 : 0) | (avg ? 1 : 0);
+    const Geometry& g = P->stage[v];
+    a.band_rows = g.band_rows;
+    a.nstrips = g.nstrips;
+    a.nbands = g.nbands;
+    a.err = &P->c.scr->err;
+    PXB_CUDA(pxb::launch_re_stage<T>(a, P->mpm != 0, P->nodata != nullptr, avg != nullptr, g.grid, s));
+    return PXB_OK;
+}
+
+template <class T>
+int re_init_impl(pxb_re_plan* P, const pxb_re_fields* f, cudaStream_t s) {
+    pxb::InitArgs<T> a{};
+    a.ny = P->c.ny;
+    a.nx = P->c.nx;
+    a.pitch = P->c.pitch;
+    a.h = (const T*)f->h;
+    a.hu = (const T*)f->hu;
+    a.hv = (const T*)f->hv;
+    a.zb = (const T*)f->z_b;
+    a.n = (const T*)f->n;
+    a.nb = (T*)f->n_b;
+    a.G = (T*)f->G;
+    a.nodata = P->nodata;
+    a.mpm = P->mpm;
+    a.sed = sed_of<T>(P);
+    PXB_CUDA(pxb::launch_re_init<T>(a, s));
+    for (auto& h : P->c.handlers) {
+        pxb::BcArgs<T> b{};
+        b.f[0] = (T*)f->h;
+        b.f[1] = (T*)f->hu;
+        b.f[2] = (T*)f->hv;
+        b.f[3] = (T*)f->z_b;
+        b.f[4] = (T*)f->n;
+        b.f[5] = (T*)f->G;
+        b.cells = h.cells;
+        b.donors = h.donors;
+        b.count = h.count;
+        b.kind = h.kind;
+        b.nx = (T)h.nx;
+        b.ny = (T)h.ny;
+        b.c0 = (T)h.c0;
+        b.c1 = (T)h.c1;
+        b.tmp = (T*)P->c.bc_tmp;
+        PXB_CUDA(pxb::launch_bc<T>(b, s));
+    }
+    return PXB_OK;
+}
+
+int re_steps(pxb_re_plan* P, const pxb_re_fields* A, const pxb_re_fields* B, int nsteps, int scheme, double cfl,
+             void* dt_log, cudaStream_t s) {
+    const bool f64 = P->c.dtype == PXB_F64;
+    auto cfl_call = [&](const pxb_re_fields* f, cudaStream_t st) {
+        return f64 ? re_cfl_impl<double>(P, f, cfl, P->c.dt_dev, dt_log, st)
+                   : re_cfl_impl<float>(P, f, cfl, P->c.dt_dev, dt_log, st);
+    };
+    auto stage_call = [&](const pxb_re_fields* in, const pxb_re_fields* out, const pxb_re_fields* avg,
+                          cudaStream_t st) {
+        return f64 ? re_stage_impl<double>(P, in, out, avg, P->c.dt_dev, st)
+                   : re_stage_impl<float>(P, in, out, avg, P->c.dt_dev, st);
+    };
+    // static planes of b are those of a
+    pxb_re_fields Bs = *B;
+    Bs.z = A->z;
+    Bs.n_b = A->n_b;
+    Bs.n = A->n;
+    const double cfl_d = cfl;
+    std::vector<const void*> key = {A->h, A->hu, A->hv, A->z_b, A->G, A->z, A->n_b, B->h, B->hu, B->hv, B->z_b,
+                                    B->G, dt_log, (const void*)(intptr_t)scheme};
+    key.push_back(*(const void* const*)&cfl_d);
+    PXB_CUDA(cudaMemsetAsync(&P->c.scr->step, 0, sizeof(unsigned int), s));
+    if (scheme == PXB_SSPRK2) {
+        pxb_re_fields B1 = Bs;
+        if (P->mpm) B1.G = nullptr;  // stage-1 G is recomputed by stage 2
+        return run_graph(P->c, key, nsteps, s, [&](cudaStream_t st) {
+            int r = cfl_call(A, st);
+            if (r == PXB_OK) r = stage_call(A, &B1, nullptr, st);
+            if (r == PXB_OK) r = stage_call(&Bs, A, A, st);
+            return r;
+        });
+    }
+    // Forward Euler: a -> b -> a pairs, then one odd step and a copy back.
+    int r = run_graph(P->c, key, nsteps / 2, s, [&](cudaStream_t st) {
+        int q = cfl_call(A, st);
+        if (q == PXB_OK) q = stage_call(A, &Bs, nullptr, st);
+        if (q == PXB_OK) q = cfl_call(&Bs, st);
+        if (q == PXB_OK) q = stage_call(&Bs, A, nullptr, st);
+        return q;
+    });
+    if (r != PXB_OK || (nsteps & 1) == 0) return r;
+    r = cfl_call(A, s);
+    if (r == PXB_OK) r = stage_call(A, &Bs, nullptr, s);
+    if (r != PXB_OK) return r;
+    const size_t es = P->c.esize();
+    const void* src[5] = {Bs.h, Bs.hu, Bs.hv, Bs.z_b, Bs.G};
+    void* dst[5] = {A->h, A->hu, A->hv, A->z_b, A->G};
+    for (int k = 0; k < 5; ++k)
+        PXB_CUDA(cudaMemcpy2DAsync(dst[k], P->c.pitch * es, src[k], P->c.pitch * es, P->c.nx * es, P->c.ny,
+                                   cudaMemcpyDeviceToDevice, s));
+    return PXB_OK;
+}
+
+// ------------------------------------------------------------------ plain Roe
+template <class T>
+int roe_cfl_impl(pxb_roe_plan* P, const pxb_roe_fields* f, double cfl, void* dt_out, void* dt_log, cudaStream_t s) {
+    pxb::CflArgs<T> a{};
+    a.ny = P->c.ny;
+    a.nx = P->c.nx;
+    a.pitch = P->c.pitch;
+    a.h = (const T*)f->h;
+    a.hu = (const T*)f->hu;
+    a.hv = (const T*)f->hv;
+    a.dx = (T)P->c.dx;
+    a.cfl = (T)cfl;
+    a.floor_dt = T(0);
+    a.scr = P->c.scr;
+    a.dt_out = (T*)dt_out;
+    a.dt_log = (T*)dt_log;
+    const long long cells = (long long)P->c.ny * P->c.nx;
+    const int grid = (int)std::max(1LL, std::min<long long>((cells + 255) / 256, 4LL * P->c.sm_count));
+    PXB_CUDA(pxb::launch_roe_cfl<T>(a, grid, s));
+    return PXB_OK;
+}
+
+template <class T>
+int roe_stage_impl(pxb_roe_plan* P, const pxb_roe_fields* in, const pxb_roe_fields* out, const pxb_roe_fields* avg,
+                   const void* dt, cudaStream_t s) {
+    pxb::RoeArgs<T> a{};
+    a.ny = P->c.ny;
+    a.nx = P->c.nx;
+    a.pitch = P->c.pitch;
+    a.dx = (T)P->c.dx;
+    a.h = (const T*)in->h;
+    a.hu = (const T*)in->hu;
+    a.hv = (const T*)in->hv;
+    a.z = (const T*)in->z;
+    a.n = (const T*)in->n;
+    a.oh = (T*)out->h;
+    a.ohu = (T*)out->hu;
+    a.ohv = (T*)out->hv;
+    a.oz = (T*)out->z;
+    a.on = (T*)out->n;
+    if (avg) {
+        a.ah = (const T*)avg->h;
+        a.ahu = (const T*)avg->hu;
+        a.ahv = (const T*)avg->hv;
+        a.az = (const T*)avg->z;
+        a.an = (const T*)avg->n;
+    }
+    a.dt = (const T*)dt;
+    a.ring = P->c.ring;
+    a.err = &P->c.scr->err;
+    PXB_CUDA(pxb::launch_roe_stage<T>(a, avg != nullptr, s));
+    return PXB_OK;
+}
+
+int check_roe_fields(const pxb_roe_fields* f) {
+    if (!f || !f->h || !f->hu || !f->hv || !f->z || !f->n) return fail(PXB_ERR_ARG, "h, hu, hv, z and n must be set");
+    return PXB_OK;
+}
+
+}  // namespace
+
+// ===================================================================== C entry points
+extern "C" {
+
+const char* pxb_last_error(void) { return g_err.c_str(); }
+int pxb_version(void) { return 1; }
+
+int pxb_re_plan_create(const pxb_re_config* cfg, pxb_re_plan** out) {
+    if (!cfg || !out) return fail(PXB_ERR_ARG, "null config or output pointer");
+    *out = nullptr;
+    if (cfg->mpm && (!cfg->seds || cfg->nsed < 1 || cfg->nsed > PXB_MAX_SED))
+        return fail(PXB_ERR_ARG, "MPM needs 1..8 sediment classes");
+    pxb_re_plan* P = new pxb_re_plan();
+    int st = common_setup(P->c, cfg->ny, cfg->nx, cfg->pitch, cfg->dtype, cfg->dx, cfg->handlers, cfg->nhandlers, false);
+    if (st != PXB_OK) {
+        P->c.release();
+        delete P;
+        return st;
+    }
+    P->mpm = cfg->mpm;
+    P->nodata = cfg->nodata;
+    P->want_rows = cfg->band_rows;
+    if (cfg->mpm) {
+        fill_sed(P->sedf, cfg->seds, cfg->nsed);
+        fill_sed(P->sedd, cfg->seds, cfg->nsed);
+    }
+    const bool f64 = cfg->dtype == PXB_F64;
+    for (int v = 0; v < 8; ++v) {
+        const bool mpm = v & 4, hm = v & 2, avg = v & 1;
+        const int bps = f64 ? pxb::re_stage_blocks_per_sm<double>(mpm, hm, avg)
+                            : pxb::re_stage_blocks_per_sm<float>(mpm, hm, avg);
+        P->stage[v] = stage_geometry(cfg->ny, cfg->nx, std::max(1, bps) * 4 * P->c.sm_count, cfg->band_rows);
+    }
+    const int cb = f64 ? pxb::re_cfl_blocks_per_sm<double>(cfg->nodata != nullptr)
+                       : pxb::re_cfl_blocks_per_sm<float>(cfg->nodata != nullptr);
+    P->c.cfl = cfl_geometry(cfg->ny, cfg->nx, std::max(1, cb) * 8 * P->c.sm_count);
+    *out = P;
+    return PXB_OK;
+}
+
+int pxb_re_plan_destroy(pxb_re_plan* plan) {
+    if (!plan) return PXB_OK;
+    cudaDeviceSynchronize();
+    plan->c.release();
+    delete plan;
+    return PXB_OK;
+}
+
+int pxb_re_init(pxb_re_plan* P, const pxb_re_fields* f, void* stream) {
+    if (!P) return fail(PXB_ERR_ARG, "null plan");
+    int st = check_fields(f, true);
+    if (st) return st;
+    if (!f->n || !f->n_b) return fail(PXB_ERR_ARG, "n and n_b must be set");
+    cudaStream_t s = (cudaStream_t)stream;
+    return P->c.dtype == PXB_F64 ? re_init_impl<double>(P, f, s) : re_init_impl<float>(P, f, s);
+}
+
+int pxb_re_cfl(pxb_re_plan* P, const pxb_re_fields* f, double cfl, void* dt_dev, void* stream) {
+    if (!P) return fail(PXB_ERR_ARG, "null plan");
+    int st = check_fields(f, true);
+    if (st) return st;
+    if (!dt_dev) return fail(PXB_ERR_ARG, "dt_dev is null");
+    cudaStream_t s = (cudaStream_t)stream;
+    return P->c.dtype == PXB_F64 ? re_cfl_impl<double>(P, f, cfl, dt_dev, nullptr, s)
+                                 : re_cfl_impl<float>(P, f, cfl, dt_dev, nullptr, s);
+}
+
+int pxb_re_stage(pxb_re_plan* P, const pxb_re_fields* in, const pxb_re_fields* out, const pxb_re_fields* avg,
+                 const void* dt_dev, void* stream) {
+    if (!P) return fail(PXB_ERR_ARG, "null plan");
+    int st = check_fields(in, !P->mpm);
+    if (st) return st;
+    st = check_fields(out, !P->mpm);
+    if (st) return st;
+    if (!in->z || !in->n_b) return fail(PXB_ERR_ARG, "input z and n_b must be set");
+    if (avg && (st = check_fields(avg, out->G != nullptr))) return st;
+    if (!dt_dev) return fail(PXB_ERR_ARG, "dt_dev is null");
+    if (in->h == out->h || in->hu == out->hu || in->hv == out->hv || in->z_b == out->z_b)
+        return fail(PXB_ERR_ARG, "stage output must not alias its input");
+    cudaStream_t s = (cudaStream_t)stream;
+    return P->c.dtype == PXB_F64 ? re_stage_impl<double>(P, in, out, avg, dt_dev, s)
+                                 : re_stage_impl<float>(P, in, out, avg, dt_dev, s);
+}
+
+int pxb_re_run(pxb_re_plan* P, const pxb_re_fields* a, const pxb_re_fields* b, int32_t nsteps, int32_t scheme,
+               double cfl, void* dt_log, void* stream) {
+    if (!P) return fail(PXB_ERR_ARG, "null plan");
+    int st = check_fields(a, true);
+    if (st) return st;
+    st = check_fields(b, true);
+    if (st) return st;
+    if (!a->z || !a->n_b) return fail(PXB_ERR_ARG, "z and n_b must be set");
+    if (nsteps < 0) return fail(PXB_ERR_ARG, "nsteps < 0");
+    if (scheme != PXB_FE && scheme != PXB_SSPRK2) return fail(PXB_ERR_ARG, "scheme must be PXB_FE or PXB_SSPRK2");
+    if (nsteps == 0) return PXB_OK;
+    return re_steps(P, a, b, nsteps, scheme, cfl, dt_log, (cudaStream_t)stream);
+}
+
+int pxb_re_check(pxb_re_plan* P, void* stream) {
+    if (!P) return fail(PXB_ERR_ARG, "null plan");
+    return check_plan_error(P->c, (cudaStream_t)stream);
+}
+
+int pxb_roe_plan_create(const pxb_roe_config* cfg, pxb_roe_plan** out) {
+    if (!cfg || !out) return fail(PXB_ERR_ARG, "null config or output pointer");
+    *out = nullptr;
+    pxb_roe_plan* P = new pxb_roe_plan();
+    int st = common_setup(P->c, cfg->ny, cfg->nx, cfg->pitch, cfg->dtype, cfg->dx, cfg->handlers, cfg->nhandlers, true);
+    if (st != PXB_OK) {
+        P->c.release();
+        delete P;
+        return st;
+    }
+    *out = P;
+    return PXB_OK;
+}
+
+int pxb_roe_plan_destroy(pxb_roe_plan* plan) {
+    if (!plan) return PXB_OK;
+    cudaDeviceSynchronize();
+    plan->c.release();
+    delete plan;
+    return PXB_OK;
+}
+
+int pxb_roe_cfl(pxb_roe_plan* P, const pxb_roe_fields* f, double cfl, void* dt_dev, void* stream) {
+    if (!P) return fail(PXB_ERR_ARG, "null plan");
+    int st = check_roe_fields(f);
+    if (st) return st;
+    if (!dt_dev) return fail(PXB_ERR_ARG, "dt_dev is null");
+    cudaStream_t s = (cudaStream_t)stream;
+    return P->c.dtype == PXB_F64 ? roe_cfl_impl<double>(P, f, cfl, dt_dev, nullptr, s)
+                                 : roe_cfl_impl<float>(P, f, cfl, dt_dev, nullptr, s);
+}
+
+int pxb_roe_stage(pxb_roe_plan* P, const pxb_roe_fields* in, const pxb_roe_fields* out, const pxb_roe_fields* avg,
+                  const void* dt_dev, void* stream) {
+    if (!P) return fail(PXB_ERR_ARG, "null plan");
+    int st = check_roe_fields(in);
+    if (st) return st;
+    st = check_roe_fields(out);
+    if (st) return st;
+    if (avg && (st = check_roe_fields(avg))) return st;
+    if (!dt_dev) return fail(PXB_ERR_ARG, "dt_dev is null");
+    if (in->h == out->h || in->hu == out->hu || in->hv == out->hv)
+        return fail(PXB_ERR_ARG, "stage output must not alias its input");
+    cudaStream_t s = (cudaStream_t)stream;
+    return P->c.dtype == PXB_F64 ? roe_stage_impl<double>(P, in, out, avg, dt_dev, s)
+                                 : roe_stage_impl<float>(P, in, out, avg, dt_dev, s);
+}
+
+int pxb_roe_run(pxb_roe_plan* P, const pxb_roe_fields* A, const pxb_roe_fields* B, int32_t nsteps, int32_t scheme,
+                double cfl, void* dt_log, void* stream) {
+    if (!P) return fail(PXB_ERR_ARG, "null plan");
+    int st = check_roe_fields(A);
+    if (st) return st;
+    st = check_roe_fields(B);
+    if (st) return st;
+    if (nsteps < 0) return fail(PXB_ERR_ARG, "nsteps < 0");
+    if (scheme != PXB_FE && scheme != PXB_SSPRK2) return fail(PXB_ERR_ARG, "scheme must be PXB_FE or PXB_SSPRK2");
+    if (nsteps == 0) return PXB_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    const bool f64 = P->c.dtype == PXB_F64;
+    const size_t es = P->c.esize();
+    // b's z and n start as copies of a's (only ring cells are rewritten by a stage)
+    PXB_CUDA(cudaMemcpy2DAsync(B->z, P->c.pitch * es, A->z, P->c.pitch * es, P->c.nx * es, P->c.ny,
+                               cudaMemcpyDeviceToDevice, s));
+    PXB_CUDA(cudaMemcpy2DAsync(B->n, P->c.pitch * es, A->n, P->c.pitch * es, P->c.nx * es, P->c.ny,
+                               cudaMemcpyDeviceToDevice, s));
+    PXB_CUDA(cudaMemsetAsync(&P->c.scr->step, 0, sizeof(unsigned int), s));
+    auto cfl_call = [&](const pxb_roe_fields* f, cudaStream_t st2) {
+        return f64 ? roe_cfl_impl<double>(P, f, cfl, P->c.dt_dev, dt_log, st2)
+                   : roe_cfl_impl<float>(P, f, cfl, P->c.dt_dev, dt_log, st2);
+    };
+    auto stage_call = [&](const pxb_roe_fields* in, const pxb_roe_fields* out, const pxb_roe_fields* avg,
+                          cudaStream_t st2) {
+        return f64 ? roe_stage_impl<double>(P, in, out, avg, P->c.dt_dev, st2)
+                   : roe_stage_impl<float>(P, in, out, avg, P->c.dt_dev, st2);
+    };
+    const double cfl_d = cfl;
+    std::vector<const void*> key = {A->h, A->hu, A->hv, A->z, A->n, B->h, B->hu, B->hv, B->z, B->n, dt_log,
+                                    (const void*)(intptr_t)scheme};
+    key.push_back(*(const void* const*)&cfl_d);
+    if (scheme == PXB_SSPRK2) {
+        return run_graph(P->c, key, nsteps, s, [&](cudaStream_t st2) {
+            int r = cfl_call(A, st2);
+            if (r == PXB_OK) r = stage_call(A, B, nullptr, st2);
+            if (r == PXB_OK) r = stage_call(B, A, A, st2);
+            return r;
+        });
+    }
+    int r = run_graph(P->c, key, nsteps / 2, s, [&](cudaStream_t st2) {
+        int q = cfl_call(A, st2);
+        if (q == PXB_OK) q = stage_call(A, B, nullptr, st2);
+        if (q == PXB_OK) q = cfl_call(B, st2);
+        if (q == PXB_OK) q = stage_call(B, A, nullptr, st2);
+        return q;
+    });
+    if (r != PXB_OK || (nsteps & 1) == 0) return r;
+    r = cfl_call(A, s);
+    if (r == PXB_OK) r = stage_call(A, B, nullptr, s);
+    if (r != PXB_OK) return r;
+    const void* src[5] = {B->h, B->hu, B->hv, B->z, B->n};
+    void* dst[5] = {A->h, A->hu, A->hv, A->z, A->n};
+    for (int k = 0; k < 5; ++k)
+        PXB_CUDA(cudaMemcpy2DAsync(dst[k], P->c.pitch * es, src[k], P->c.pitch * es, P->c.nx * es, P->c.ny,
+                                   cudaMemcpyDeviceToDevice, s));
+    return PXB_OK;
+}
+
+int pxb_roe_check(pxb_roe_plan* P, void* stream) {
+    if (!P) return fail(PXB_ERR_ARG, "null plan");
+    return check_plan_error(P->c, (cudaStream_t)stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,336 @@
+// Device-side building blocks of the PyExner B200 step: constants, NaN-faithful
+// helpers, per-cell precomputes and the per-face Riemann / bedload / wave-speed math.
+//
+// The arithmetic follows the reference expression by expression (operation order,
+// clamps, masks) so that the float64 build, compiled with --fmad=false, reproduces the
+// reference to rounding of the transcendental functions.  Citations are to PyExner's
+// src/PyExner/solvers/kernels/roe_exner.py unless stated otherwise.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "pxb_types.h"
+
+namespace pxb {
+
+constexpr double G_ACC = 9.81;     // src/utils/constants.py:33
+constexpr double DRY_TOL = 1e-4;   // constants.py:29
+constexpr double SED_TOL = 1e-5;   // constants.py:30
+constexpr double VEL_TOL = 1e-6;   // constants.py:31
+constexpr double DT_FLOOR = 1e-6;  // roe_exner_solver.py:121
+constexpr double TWO_PI = 6.283185307179586;  // 2*jnp.pi as a Python float
+constexpr unsigned FULL = 0xffffffffu;
+
+// jnp.maximum(x, lo) for a constant lo: NaN in x propagates.
+template <class T>
+__device__ __forceinline__ T clamp_lo(T x, T lo) { return x < lo ? lo : x; }
+// jnp.maximum(a, b) with NaN from either side.
+template <class T>
+__device__ __forceinline__ T nan_max(T a, T b) { return (a < b || b != b) ? b : a; }
+// jnp.clip(x, -1, 1) keeping NaN.
+template <class T>
+__device__ __forceinline__ T clip1(T x) { return x < T(-1) ? T(-1) : (x > T(1) ? T(1) : x); }
+
+__device__ __forceinline__ float d_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double d_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float d_cbrt(float x) { return cbrtf(x); }
+__device__ __forceinline__ double d_cbrt(double x) { return cbrt(x); }
+__device__ __forceinline__ float d_pow(float x, float y) { return powf(x, y); }
+__device__ __forceinline__ double d_pow(double x, double y) { return pow(x, y); }
+__device__ __forceinline__ float d_acos(float x) { return acosf(x); }
+__device__ __forceinline__ double d_acos(double x) { return acos(x); }
+__device__ __forceinline__ float d_cos(float x) { return cosf(x); }
+__device__ __forceinline__ double d_cos(double x) { return cos(x); }
+__device__ __forceinline__ bool d_isfinite(float x) { return isfinite(x); }
+__device__ __forceinline__ bool d_isfinite(double x) { return isfinite(x); }
+
+// ---------------------------------------------------------------- hydrodynamic faces
+// Per-cell values used by the Roe-Exner face flux (roe_exner.py:317-335, 421-425, 455).
+template <class T>
+struct HCell {
+    T h;   // max(h, DRY_TOL)
+    T u;   // hu / h if wet else 0
+    T v;
+    T sq;  // sqrt(h)
+    T c;   // sqrt(g h)
+    T zt;  // z + z_b with z_b floored at SED_TOL*0.01 below SED_TOL
+    T nb;  // n_b
+};
+
+template <class T>
+__device__ __forceinline__ HCell<T> make_hcell(T h, T hu, T hv, T zb, T z, T nb) {
+    HCell<T> p;
+    const T hc = clamp_lo(h, T(DRY_TOL));
+    const bool wet = hc > T(DRY_TOL);
+    p.h = hc;
+    p.u = wet ? hu / hc : T(0);
+    p.v = wet ? hv / hc : T(0);
+    p.sq = d_sqrt(hc);
+    p.c = d_sqrt(T(G_ACC) * hc);
+    const T zbc = zb > T(SED_TOL) ? zb : T(SED_TOL * 0.01);
+    p.zt = z + zbc;
+    p.nb = nb;
+    return p;
+}
+
+// Roe-Exner fluctuations of one face (roe_exner.py:312-533).  YF selects the y-face
+// orientation (normal (0,-1): normal velocity -v, tangential u); otherwise (1,0).
+// Outputs upwP (to cell j) and upwM (to cell i) in (h, hu, hv).
+template <class T, bool YF>
+__device__ __forceinline__ void roe_exner_face(const HCell<T>& I, const HCell<T>& J, T dx, T P[3], T M[3]) {
+    const T uhi = YF ? -I.v : I.u, vhi = YF ? I.u : I.v;
+    const T uhj = YF ? -J.v : J.u, vhj = YF ? J.u : J.v;
+    const T den = I.sq + J.sq;
+    const T ht = T(0.5) * (I.h + J.h);
+    const T ct = d_sqrt(T(G_ACC) * ht);
+    const T ut = (uhi * I.sq + uhj * J.sq) / den;
+    const T vt = (vhi * I.sq + vhj * J.sq) / den;
+    const T l1r = ut - ct;
+    const T l3r = ut + ct;
+    // Harten-Hyman (roe_exner.py:357-371); the VEL_TOL guard only in the lambda_3 speed
+    T l1 = l1r, lE1 = T(0);
+    const T ei = uhi - I.c, ej = uhj - J.c;
+    const bool m1 = (ei < T(0)) && (ej > T(0));
+    if (m1) {
+        const T t = ei * (ej - l1r) / (ej - ei);
+        lE1 = l1r - t;
+        l1 = t;
+    }
+    T l3 = l3r, lE3 = T(0);
+    const T fi = uhi + I.c, fj = uhj + J.c;
+    const bool m3 = (fi < T(0)) && (fj > T(0));
+    if (m3) {
+        const T num = fj * (l3r - fi);
+        lE3 = l3r - num / (fj - fi);
+        l3 = num / ((fj - fi) + T(VEL_TOL));
+    }
+    const T dh = J.h - I.h;
+    const T dhu = J.h * uhj - I.h * uhi;
+    const T dhv = J.h * vhj - I.h * vhi;
+    const T den2 = T(-2.0) * ct;
+    const T a1 = (-l3r * dh + dhu) / den2;
+    const T a2 = (-vt * dh + dhv) / ct;
+    const T a3 = (l1r * dh - dhu) / den2;
+    const T dz = J.zt - I.zt;
+    const T thrust = -T(G_ACC) * ht * dz;
+    const T nt = T(0.5) * (I.nb + J.nb);
+    const T sf = (nt * nt * d_sqrt(ut * ut + vt * vt) * ut) / clamp_lo(d_pow(ht, T(4.0 / 3.0)), T(DRY_TOL));
+    const T tau = T(G_ACC) * ht * sf * dx;
+    const T b1 = (thrust - tau) / den2;
+    const T b3 = -b1;
+    // Upwinded waves (roe_exner.py:484-507); P columns (1,l1,vt), (0,0,ct), (1,l3,vt).
+    T p0 = T(0), p1 = T(0), p2 = T(0), n0 = T(0), n1 = T(0), n2 = T(0);
+    {
+        const T w = l1 * a1 - b1;
+        if (l1 > T(0)) { p0 = p0 + w; p1 = p1 + w * l1; p2 = p2 + w * vt; }
+        else if (l1 <= T(0)) { n0 = n0 + w; n1 = n1 + w * l1; n2 = n2 + w * vt; }
+    }
+    {
+        const T w = ut * a2;  // beta_2 = 0
+        if (ut > T(0)) p2 = p2 + w * ct;
+        else if (ut <= T(0)) n2 = n2 + w * ct;
+    }
+    {
+        const T w = l3 * a3 - b3;
+        if (l3 > T(0)) { p0 = p0 + w; p1 = p1 + w * l3; p2 = p2 + w * vt; }
+        else if (l3 <= T(0)) { n0 = n0 + w; n1 = n1 + w * l3; n2 = n2 + w * vt; }
+    }
+    // Entropy-fix waves (roe_exner.py:510-524); lambda_E2 = 0 adds nothing.
+    if (m1) {
+        const T e = lE1 * a1;
+        if (lE1 > T(0)) { p0 = p0 + e; p1 = p1 + e * l1; p2 = p2 + e * vt; }
+        else if (lE1 <= T(0)) { n0 = n0 + e; n1 = n1 + e * l1; n2 = n2 + e * vt; }
+    }
+    if (m3) {
+        const T e = lE3 * a3;
+        if (lE3 > T(0)) { p0 = p0 + e; p1 = p1 + e * l3; p2 = p2 + e * vt; }
+        else if (lE3 <= T(0)) { n0 = n0 + e; n1 = n1 + e * l3; n2 = n2 + e * vt; }
+    }
+    // back to (x, y) (roe_exner.py:526-531)
+    if (YF) {
+        P[0] = p0; P[1] = p2; P[2] = -p1;
+        M[0] = n0; M[1] = n2; M[2] = -n1;
+    } else {
+        P[0] = p0; P[1] = p1; P[2] = p2;
+        M[0] = n0; M[1] = n1; M[2] = n2;
+    }
+}
+
+// ----------------------------------------------------------------------- bedload
+// Per-cell values of the Exner face (roe_exner.py:620-646).
+template <class T>
+struct ECell {
+    T h;   // depth as stored (activity test)
+    T zb;  // z_b as stored (activity test, update base)
+    T zbe; // floored z_b
+    T sq;  // sqrt(floored h)
+    T u, v, um;  // velocity, |u|^2
+    T G;
+};
+
+template <class T>
+__device__ __forceinline__ ECell<T> make_ecell(T h, T hu, T hv, T zb, T G) {
+    ECell<T> e;
+    const T he = h > T(DRY_TOL) ? h : T(DRY_TOL * 0.01);
+    const bool wet = he > T(DRY_TOL);
+    e.h = h;
+    e.zb = zb;
+    e.zbe = zb > T(SED_TOL) ? zb : T(SED_TOL * 0.01);
+    e.sq = d_sqrt(he);
+    e.u = wet ? hu / he : T(0);
+    e.v = wet ? hv / he : T(0);
+    e.um = e.u * e.u + e.v * e.v;
+    e.G = G;
+    return e;
+}
+
+template <class T, bool YF>
+__device__ __forceinline__ T exner_face(const ECell<T>& I, const ECell<T>& J) {
+    const T uhi = YF ? -I.v : I.u;
+    const T uhj = YF ? -J.v : J.u;
+    const T ut = (uhi * I.sq + uhj * J.sq) / (I.sq + J.sq);
+    const T qi = I.G * I.um * uhi;
+    const T qj = J.G * J.um * uhj;
+    const T gt = T(0.5) * (I.G + J.G);
+    const T dz = J.zbe - I.zbe;
+    const T dq = gt * J.um * uhj - gt * I.um * uhi;
+    const T lam4 = fabs(dz) > T(SED_TOL) ? dq / dz : ut;
+    const T qbi = qi + (gt - I.G) * I.um * uhi;
+    const T qbj = qj + (gt - J.G) * J.um * uhj;
+    return lam4 >= T(0) ? qbi : qbj;
+}
+
+// Exner face activity (roe_exner.py:687-701): wet on either side, neither side nodata,
+// and not both sediment layers below SED_TOL.
+template <class T>
+__device__ __forceinline__ bool exner_active(const ECell<T>& I, const ECell<T>& J, bool mi, bool mj) {
+    return ((I.h > T(DRY_TOL)) || (J.h > T(DRY_TOL))) && !(mi || mj) &&
+           !((I.zb < T(SED_TOL)) && (J.zb < T(SED_TOL)));
+}
+
+// ----------------------------------------------------------------- grass factor
+template <class T>
+struct SedT {
+    T np2;    // n_p^2
+    T sm1d;   // (s - 1) d50
+    T thc;    // theta_c
+    T np3sg;  // n_p^3 sqrt(g)
+    T sm1;    // s - 1
+    T frac;
+};
+
+template <class T>
+struct SedTable {
+    SedT<T> s[PXB_MAX_SED];
+    int n;
+    T one_minus_por;  // 1 - mean(porosity)
+    T n_p_mix;        // (mean(d50*frac))^(1/6) / 21.1   (compute_n)
+};
+
+// Meyer-Peter & Mueller grass factor of one cell (roe_exner.py:85-130).
+template <class T>
+__device__ __forceinline__ T mpm_grass(T h, T hu, T hv, bool nodata, const SedTable<T>& S) {
+    const T hc = clamp_lo(h, T(DRY_TOL));
+    const T u = hu / hc, v = hv / hc;
+    const T vel2 = u * u + v * v;
+    const T cb = d_cbrt(hc);
+    const T sqh = d_sqrt(hc);
+    T G = T(0);
+    for (int k = 0; k < S.n; ++k) {
+        const SedT<T>& s = S.s[k];
+        T theta = (s.np2 * vel2) / (s.sm1d * cb);
+        theta = clamp_lo(theta, T(0));
+        const T dth = clamp_lo(theta - s.thc, T(0));
+        const T g1 = s.np3sg / (s.sm1 * sqh);
+        const T g2 = T(8.0) * d_sqrt(dth) / (d_pow(theta, T(1.5)) + T(1e-5));
+        const T contrib = s.frac * g1 * g2 * dth;
+        G = (k == 0) ? contrib : G + contrib;
+    }
+    G = G / S.one_minus_por;
+    if (nodata) G = T(0);
+    return hc > T(DRY_TOL) ? G : T(0);
+}
+
+// Constant grass factor pass-through (roe_exner.py:136-140).
+template <class T>
+__device__ __forceinline__ T const_grass(T h, T G, bool nodata) {
+    if (nodata) G = T(0);
+    return h > T(DRY_TOL) ? G : T(0);
+}
+
+// ------------------------------------------------------------------ wave speeds
+template <class T>
+struct CCell {
+    T h;  // max(h, DRY_TOL)
+    T sq, u, v, G;
+};
+
+template <class T>
+__device__ __forceinline__ CCell<T> make_ccell(T h, T hu, T hv, T G) {
+    CCell<T> p;
+    p.h = clamp_lo(h, T(DRY_TOL));
+    p.sq = d_sqrt(p.h);
+    p.u = hu / p.h;
+    p.v = hv / p.h;
+    p.G = G;
+    return p;
+}
+
+// Extreme roots of the coupled cubic (roe_exner.py:163-209), trigonometric Cardano,
+// with the linear speeds when a < 1e-5.
+template <class T>
+__device__ __forceinline__ void cubic_extremes(T ut, T at, T ct, T& lmin, T& lmax) {
+    if (at < T(1e-5)) {
+        lmin = ut - ct;
+        lmax = ut + ct;
+        return;
+    }
+    const T b = T(-2) * ut;
+    const T c = (T(1) + at) * (ct * ct) - ut * ut;
+    const T d = -(ct * ct) * at * ut;
+    const T p = (T(-3) * c - b * b) / T(3);
+    const T q = (T(2) * d_pow(b, T(3)) - T(-9) * b * c + T(27) * d) / T(-27);
+    const T x = clip1((T(3) * q) / (T(2) * p) * d_sqrt(T(-3) / p));
+    const T th = d_acos(x);
+    const T sq = T(2) * d_sqrt(-p / T(3));
+    const T shift = -b / T(-3);
+    lmax = sq * d_cos(th / T(3)) + shift;
+    lmin = sq * d_cos((th + T(TWO_PI)) / T(3)) + shift;
+}
+
+// Largest characteristic speed of one face (roe_exner.py:211-255); the face step is
+// dx / speed, so the global minimum step is dx / (maximum speed).
+template <class T, bool YF>
+__device__ __forceinline__ T face_speed(const CCell<T>& I, const CCell<T>& J) {
+    const T uhi = YF ? -I.v : I.u, vhi = YF ? I.u : I.v;
+    const T uhj = YF ? -J.v : J.u, vhj = YF ? J.u : J.v;
+    const T den = I.sq + J.sq;
+    const T ht = T(0.5) * (I.h + J.h);
+    const T ut = (uhi * I.sq + uhj * J.sq) / den;
+    const T ct = d_sqrt(T(G_ACC) * ht);
+    const T gt = T(0.5) * (I.G + J.G);
+    const T at = gt * (uhi * uhi + uhi * uhj + uhj * uhj + vhi * vhj) / (I.sq * J.sq);
+    const T l1 = ut - ct, l3 = ut + ct;
+    T lmin, lmax;
+    cubic_extremes(ut, at, ct, lmin, lmax);
+    const T roe = nan_max(fabs(lmin), fabs(lmax));
+    const T swe = nan_max(fabs(l1), fabs(l3));
+    return roe < T(VEL_TOL) ? swe : roe;
+}
+
+// Order-preserving map of a non-negative (or NaN) float to unsigned bits for atomicMax.
+__device__ __forceinline__ unsigned long long speed_bits(double s) { return (unsigned long long)__double_as_longlong(s); }
+__device__ __forceinline__ unsigned long long speed_bits(float s) { return (unsigned long long)(unsigned)__float_as_uint(s); }
+__device__ __forceinline__ double bits_speed(unsigned long long b, double) { return __longlong_as_double((long long)b); }
+__device__ __forceinline__ float bits_speed(unsigned long long b, float) { return __uint_as_float((unsigned)b); }
+
+// ----------------------------------------------------------------- ring recipes
+__device__ __forceinline__ int ring_slot(int r, int c, int ny, int nx) {
+    if (r == 0) return c;
+    if (r == ny - 1) return nx + c;
+    if (c == 0) return 2 * nx + r;
+    if (c == nx - 1) return 2 * nx + ny + r;
+    return -1;
+}
+
+}  // namespace pxb

@@ -1,0 +1,29 @@
+// Launch entry points implemented per precision (kernels_f32.cu, kernels_f64.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "init_bc.cuh"
+#include "re_cfl.cuh"
+#include "re_stage.cuh"
+#include "roe_plain.cuh"
+
+namespace pxb {
+
+template <class T>
+cudaError_t launch_re_stage(const REStageArgs<T>& a, bool mpm, bool has_mask, bool avg, int grid, cudaStream_t s);
+template <class T>
+int re_stage_blocks_per_sm(bool mpm, bool has_mask, bool avg);
+template <class T>
+cudaError_t launch_re_cfl(const CflArgs<T>& a, bool has_mask, int grid, cudaStream_t s);
+template <class T>
+int re_cfl_blocks_per_sm(bool has_mask);
+template <class T>
+cudaError_t launch_re_init(const InitArgs<T>& a, cudaStream_t s);
+template <class T>
+cudaError_t launch_bc(const BcArgs<T>& a, cudaStream_t s);
+template <class T>
+cudaError_t launch_roe_stage(const RoeArgs<T>& a, bool avg, cudaStream_t s);
+template <class T>
+cudaError_t launch_roe_cfl(const CflArgs<T>& a, int grid, cudaStream_t s);
+
+}  // namespace pxb

@@ -1,0 +1,130 @@
+// CFL reduction for the Roe-Exner bundle (compute_dt_roeexner,
+// PyExner src/PyExner/solvers/roe_exner_solver.py:118-122 with compute_dt_2D,
+// roe_exner.py:257-310).
+//
+// min over active faces of dx / speed_f equals dx / max_f speed_f exactly (division by
+// a positive number is monotone under round-to-nearest), so the kernel reduces the
+// maximum speed: a warp-level max of the IEEE bit patterns (speeds are >= 0 or NaN, so
+// unsigned order is float order and NaN wins like jnp.min's NaN), one 64-bit atomicMax
+// per warp, and the last block to finish turns it into dt = max(cfl * dx / smax, 1e-6),
+// resets the accumulator and logs dt.  Deterministic and free of host round trips.
+//
+// Work layout: a warp covers 32 columns and the 31 x-faces between them (strips overlap
+// by one column) and marches down a band of rows; y-faces (r | r+1) belong to row r's band.
+#pragma once
+#include "pxb_device.cuh"
+
+namespace pxb {
+
+struct CflScratch {
+    unsigned long long maxbits;  // running max of speed bits
+    unsigned int done;           // finished blocks of the current launch
+    unsigned int step;           // index into the dt log
+    int err;                     // sticky error word
+    int pad;
+};
+
+template <class T>
+struct CflArgs {
+    int ny, nx;
+    long long pitch;
+    const T *h, *hu, *hv, *G;
+    const uint8_t* nodata;
+    T dx, cfl, floor_dt;  // floor_dt = 1e-6 (Roe-Exner); <= 0 disables the floor
+    CflScratch* scr;
+    T* dt_out;   // device scalar
+    T* dt_log;   // optional: dt_log[scr->step++] = dt
+    int band_rows, nstrips, nbands;
+};
+
+template <class T, bool HAS_MASK>
+__global__ void __launch_bounds__(256) re_cfl_kernel(const CflArgs<T> a) {
+    const int lane = threadIdx.x & 31;
+    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    const int ny = a.ny, nx = a.nx;
+    const T DRY = T(DRY_TOL);
+    unsigned long long best = 0ull;
+    const int nitems = a.nstrips * a.nbands;
+    for (int item = wid; item < nitems; item += nw) {
+        const int band = item / a.nstrips;
+        const int strip = item - band * a.nstrips;
+        const int c = strip * 31 + lane;
+        const bool colok = c < nx;
+        const bool has_e = colok && (c + 1 < nx) && lane < 31;
+        const int R0 = band * a.band_rows;
+        const int R1 = min(ny, R0 + a.band_rows);
+        CCell<T> prev = make_ccell(T(1), T(0), T(0), T(0));
+        T hprev = 0;
+        bool mprev = false;
+        for (int r = R0; r < min(ny, R1 + 1); ++r) {
+            T h = 1, hu = 0, hv = 0, g = 0;
+            bool m = false;
+            if (colok) {
+                const long long i = (long long)r * a.pitch + c;
+                h = a.h[i];
+                hu = a.hu[i];
+                hv = a.hv[i];
+                g = a.G[i];
+                if (HAS_MASK) m = a.nodata[i] != 0;
+            }
+            const CCell<T> cur = make_ccell(h, hu, hv, g);
+            if (r < R1) {  // x-face (c | c+1) of row r
+                CCell<T> e;
+                e.h = __shfl_down_sync(FULL, cur.h, 1);
+                e.sq = __shfl_down_sync(FULL, cur.sq, 1);
+                e.u = __shfl_down_sync(FULL, cur.u, 1);
+                e.v = __shfl_down_sync(FULL, cur.v, 1);
+                e.G = __shfl_down_sync(FULL, cur.G, 1);
+                const T he = __shfl_down_sync(FULL, h, 1);
+                const bool me = HAS_MASK ? (__shfl_down_sync(FULL, (int)m, 1) != 0) : false;
+                if (has_e && ((h > DRY) || (he > DRY)) && !(m || me)) {
+                    const unsigned long long b = speed_bits(face_speed<T, false>(cur, e));
+                    best = b > best ? b : best;
+                }
+            }
+            if (r > R0 && colok && ((hprev > DRY) || (h > DRY)) && !(mprev || m)) {  // y-face (r-1 | r)
+                const unsigned long long b = speed_bits(face_speed<T, true>(prev, cur));
+                best = b > best ? b : best;
+            }
+            prev = cur;
+            hprev = h;
+            mprev = m;
+        }
+    }
+    // warp max, one atomic per warp
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long other = __shfl_xor_sync(FULL, best, o);
+        best = other > best ? other : best;
+    }
+    if (lane == 0) {
+        if (best != 0ull) atomicMax(&a.scr->maxbits, best);
+        __threadfence();
+    }
+    // last block finalises
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned int ticket = atomicAdd(&a.scr->done, 1u);
+        last = (ticket == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        const unsigned long long bits = atomicAdd(&a.scr->maxbits, 0ull);
+        const T smax = bits_speed(bits, T(0));
+        // min_f dx/speed_f (inf when no face is active), then cfl * dt and the floor
+        T dt = a.cfl * (a.dx / smax);
+        if (a.floor_dt > T(0)) dt = clamp_lo(dt, a.floor_dt);
+        *a.dt_out = dt;
+        if (a.dt_log) a.dt_log[a.scr->step] = dt;
+        a.scr->step += 1;
+        if (!d_isfinite(dt)) a.scr->err |= 2;
+        a.scr->maxbits = 0ull;
+        a.scr->done = 0u;
+        __threadfence();
+    }
+}
+
+}  // namespace pxb

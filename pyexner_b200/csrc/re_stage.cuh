@@ -1,0 +1,313 @@
+// Fused Roe-Exner stage kernel (one launch per Runge-Kutta stage).
+//
+// Replaces step_fn_roeexner (PyExner src/PyExner/solvers/roe_exner_solver.py:80-116) on
+// one rank: hydro update (roe_exner.py:535-612) -> momentum corrections (:14-62) ->
+// boundary handlers -> grass factor (:85-140) -> Exner update (:665-717) -> boundary
+// handlers, and for the second SSPRK2 stage the 0.5/0.5 combination (SSPRK2.py:40).
+//
+// Layout of the work: a warp owns a strip of 32 columns (3 halo | 26 owned | 3 halo) and
+// marches down a band of rows.  Each iteration loads one new row and advances a
+// software pipeline held in registers:
+//   A  row r   : cell precompute, x-face fluxes (east neighbour by shuffle), y-face (r-1|r)
+//   B  row r-1 : hydro update (all four faces known)
+//   C  row r-2 : momentum corrections (needs updated depths of rows r-3..r-1)
+//   D  row r-3 : first boundary application on ring cells (donors in rows r-4..r-2)
+//   E  row r-3 : grass factor, Exner cell, Exner x-faces and y-face (r-4|r-3)
+//   F  row r-4 : z_b update
+//   G  row r-5 : second boundary application on z_b and G, then the z_b / G stores
+// Hydro fields are stored after D (the second application leaves them unchanged for
+// the layouts the host accepts).  Every face is evaluated once per warp; the only
+// redundant work is the 6 halo columns of each strip and 6 halo rows of each band.
+#pragma once
+#include "pxb_device.cuh"
+
+namespace pxb {
+
+template <class T>
+struct REStageArgs {
+    int ny, nx;
+    long long pitch;
+    T dx;
+    const T *h, *hu, *hv, *zb, *z, *nb, *G;  // stage input (G read in constant-G mode)
+    const uint8_t* nodata;                    // mask[0] or null
+    T *oh, *ohu, *ohv, *ozb, *oG;            // stage output (oG may be null)
+    const T *ah, *ahu, *ahv, *azb, *aG;      // SSPRK2 partner u^n (AVG)
+    const T* dt;
+    const pxb_ring_recipe* ring;              // null when there are no handlers
+    SedTable<T> sed;
+    int band_rows, nstrips, nbands;
+    int* err;
+};
+
+template <class T>
+__device__ __forceinline__ T pick_row(int dy, T above, T mid, T below) {
+    return dy < 0 ? above : (dy > 0 ? below : mid);
+}
+
+template <class T>
+__device__ __forceinline__ HCell<T> shfl_down_hcell(const HCell<T>& p) {
+    HCell<T> q;
+    q.h = __shfl_down_sync(FULL, p.h, 1);
+    q.u = __shfl_down_sync(FULL, p.u, 1);
+    q.v = __shfl_down_sync(FULL, p.v, 1);
+    q.sq = __shfl_down_sync(FULL, p.sq, 1);
+    q.c = __shfl_down_sync(FULL, p.c, 1);
+    q.zt = __shfl_down_sync(FULL, p.zt, 1);
+    q.nb = __shfl_down_sync(FULL, p.nb, 1);
+    return q;
+}
+
+template <class T>
+__device__ __forceinline__ ECell<T> shfl_down_ecell(const ECell<T>& p) {
+    ECell<T> q;
+    q.h = __shfl_down_sync(FULL, p.h, 1);
+    q.zb = __shfl_down_sync(FULL, p.zb, 1);
+    q.zbe = __shfl_down_sync(FULL, p.zbe, 1);
+    q.sq = __shfl_down_sync(FULL, p.sq, 1);
+    q.u = __shfl_down_sync(FULL, p.u, 1);
+    q.v = __shfl_down_sync(FULL, p.v, 1);
+    q.um = __shfl_down_sync(FULL, p.um, 1);
+    q.G = __shfl_down_sync(FULL, p.G, 1);
+    return q;
+}
+
+template <class T, bool MPM, bool HAS_MASK, bool AVG>
+__global__ void __launch_bounds__(128) re_stage_kernel(const REStageArgs<T> a) {
+    const int lane = threadIdx.x & 31;
+    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    const int ny = a.ny, nx = a.nx;
+    const long long pitch = a.pitch;
+    const T dt = *a.dt;
+    const T dx = a.dx;
+    const T DRY = T(DRY_TOL);
+    const int nitems = a.nstrips * a.nbands;
+    bool bad = false;
+
+    for (int item = wid; item < nitems; item += nw) {
+        const int band = item / a.nstrips;
+        const int strip = item - band * a.nstrips;
+        const int c = strip * PXB_STRIP_OUT - PXB_HALO + lane;
+        const bool colok = (c >= 0) && (c < nx);
+        const bool has_e = colok && (c + 1 < nx) && (lane < 31);
+        const bool last_strip = strip == a.nstrips - 1;
+        const bool out_col = colok && lane >= PXB_HALO && (lane < PXB_HALO + PXB_STRIP_OUT || last_strip);
+        const bool interior_col = (c >= 1) && (c <= nx - 2);
+        const int R0 = band * a.band_rows;
+        const int R1 = (band == a.nbands - 1) ? ny : R0 + a.band_rows;
+        const int L0 = max(0, R0 - 3), L1 = min(ny, R1 + 3);
+
+        // ---- carried pipeline state
+        HCell<T> pA = make_hcell(T(0), T(0), T(0), T(0), T(0), T(0));
+        T hA = 0, huA = 0, hvA = 0, ztA = 0;
+        T xfA0 = 0, xfA1 = 0, xfA2 = 0, nfA0 = 0, nfA1 = 0, nfA2 = 0;
+        T hr3 = 0, hr2 = 0, hur2 = 0, hvr2 = 0, zt3 = 0, zt2 = 0;
+        unsigned mwin = 0;  // bit k = nodata of row r-1-k
+        T zin1 = 0, zin2 = 0, zin3 = 0, zin4 = 0;
+        T gin1 = 0, gin2 = 0, gin3 = 0, gin4 = 0;
+        T hf4h = 0, hf4u = 0, hf4v = 0, hf3h = 0, hf3u = 0, hf3v = 0;
+        ECell<T> e4 = make_ecell(T(0), T(0), T(0), T(0), T(0));
+        T xe4 = 0, fn4 = 0;
+        T zbp6 = 0, zbp5 = 0, gg6 = 0, gg5 = 0;
+
+        for (int r = L0; r < L1 + 5; ++r) {
+            const bool rowA = r < L1;
+            // ================= A: load row r, x-faces of row r, y-face (r-1 | r)
+            T h_r = 0, hu_r = 0, hv_r = 0, zb_r = 0, z_r = 0, nb_r = 0, g_r = 0;
+            bool m_r = false;
+            if (rowA && colok) {
+                const long long i = (long long)r * pitch + c;
+                h_r = a.h[i];
+                hu_r = a.hu[i];
+                hv_r = a.hv[i];
+                zb_r = a.zb[i];
+                z_r = a.z[i];
+                nb_r = a.nb[i];
+                if (!MPM) g_r = a.G[i];
+                if (HAS_MASK) m_r = a.nodata[i] != 0;
+            }
+            const HCell<T> pr = make_hcell(h_r, hu_r, hv_r, zb_r, z_r, nb_r);
+            const T zt_r = z_r + zb_r;
+            T xf0 = 0, xf1 = 0, xf2 = 0;
+            {
+                const HCell<T> pe = shfl_down_hcell(pr);
+                const T he = __shfl_down_sync(FULL, h_r, 1);
+                const bool me = HAS_MASK ? (__shfl_down_sync(FULL, (int)m_r, 1) != 0) : false;
+                const bool xact = rowA && has_e && ((h_r > DRY) || (he > DRY)) && !(m_r || me);
+                T P[3] = {T(0), T(0), T(0)}, M[3] = {T(0), T(0), T(0)};
+                if (xact) roe_exner_face<T, false>(pr, pe, dx, P, M);
+                const T w0 = __shfl_up_sync(FULL, P[0], 1);
+                const T w1 = __shfl_up_sync(FULL, P[1], 1);
+                const T w2 = __shfl_up_sync(FULL, P[2], 1);
+                const bool wact = (__shfl_up_sync(FULL, (int)xact, 1) != 0) && lane > 0;
+                // scatter order of roe_exner.py:599-600: east upwM first, then west upwP
+                if (xact) { xf0 = xf0 + M[0]; xf1 = xf1 + M[1]; xf2 = xf2 + M[2]; }
+                if (wact) { xf0 = xf0 + w0; xf1 = xf1 + w1; xf2 = xf2 + w2; }
+            }
+            T yP[3] = {T(0), T(0), T(0)}, yM[3] = {T(0), T(0), T(0)};
+            const bool yact = rowA && (r - 1 >= L0) && colok && ((hA > DRY) || (h_r > DRY)) && !((mwin & 1u) || m_r);
+            if (yact) roe_exner_face<T, true>(pA, pr, dx, yP, yM);
+
+            // ================= B: hydro update of row r-1
+            T hr1 = 0, hur1 = 0, hvr1 = 0;
+            if (r - 1 >= L0 && r - 1 < L1) {
+                T f0 = xfA0, f1 = xfA1, f2 = xfA2;
+                f0 = f0 + yM[0]; f1 = f1 + yM[1]; f2 = f2 + yM[2];      // south face upwM
+                f0 = f0 + nfA0; f1 = f1 + nfA1; f2 = f2 + nfA2;         // north face upwP
+                hr1 = hA - dt * f0 / dx;
+                hur1 = huA - dt * f1 / dx;
+                hvr1 = hvA - dt * f2 / dx;
+            }
+
+            // ================= C: momentum corrections of row r-2
+            T hf2h = 0, hf2u = 0, hf2v = 0;
+            {
+                const int q2 = r - 2;
+                const T hE = __shfl_down_sync(FULL, hr2, 1), hW = __shfl_up_sync(FULL, hr2, 1);
+                const T zE = __shfl_down_sync(FULL, zt2, 1), zW = __shfl_up_sync(FULL, zt2, 1);
+                const bool m2 = HAS_MASK && ((mwin >> 1) & 1u);
+                const bool mE = HAS_MASK ? (__shfl_down_sync(FULL, (int)m2, 1) != 0) : false;
+                const bool mW = HAS_MASK ? (__shfl_up_sync(FULL, (int)m2, 1) != 0) : false;
+                if (q2 >= L0 && q2 < L1) {
+                    hf2h = hr2;
+                    hf2u = hur2;
+                    hf2v = hvr2;
+                    if (interior_col && q2 >= 1 && q2 <= ny - 2) {
+                        const bool mN = HAS_MASK && ((mwin >> 2) & 1u);
+                        const bool mS = HAS_MASK && (mwin & 1u);
+                        const T eta = hr2 + zt2;
+                        const bool stop_u = ((eta < zE) && (hE < DRY)) || ((eta < zW) && (hW < DRY)) || mE || mW;
+                        const bool stop_v = ((eta < zt3) && (hr3 < DRY)) || ((eta < ztA) && (hr1 < DRY)) || mN || mS;
+                        const bool active = (hr2 > DRY) && !m2;
+                        hf2u = (active && !stop_u) ? hur2 : T(0);
+                        hf2v = (active && !stop_v) ? hvr2 : T(0);
+                    }
+                }
+            }
+
+            // ================= D: first boundary application on row q = r-3
+            const int q = r - 3;
+            const bool rowD = (q >= L0) && (q < L1);
+            T hbh = hf3h, hbu = hf3u, hbv = hf3v, zb1 = zin3, gb1 = gin3;
+            if (a.ring != nullptr && rowD) {
+                const int slot = colok ? ring_slot(q, c, ny, nx) : -1;
+                unsigned flags = 0;
+                int hdy = 0, hdx = 0, mdy = 0, mdx = 0, zdy = 0, zdx = 0, gdy = 0, gdx = 0;
+                T m0 = 0, m1 = 0, m2c = 0, m3 = 0;
+                if (slot >= 0) {
+                    const pxb_ring_recipe& rc = a.ring[slot];
+                    flags = rc.flags;
+                    hdy = rc.h_dy; hdx = rc.h_dx; mdy = rc.m_dy; mdx = rc.m_dx;
+                    zdy = rc.zb_dy; zdx = rc.zb_dx; gdy = rc.g_dy; gdx = rc.g_dx;
+                    m0 = T(rc.m[0]); m1 = T(rc.m[1]); m2c = T(rc.m[2]); m3 = T(rc.m[3]);
+                }
+                if (__any_sync(FULL, flags != 0)) {
+                    const T vh = __shfl_sync(FULL, pick_row(hdy, hf4h, hf3h, hf2h), lane + hdx);
+                    const T vu = __shfl_sync(FULL, pick_row(mdy, hf4u, hf3u, hf2u), lane + mdx);
+                    const T vv = __shfl_sync(FULL, pick_row(mdy, hf4v, hf3v, hf2v), lane + mdx);
+                    const T vz = __shfl_sync(FULL, pick_row(zdy, zin4, zin3, zin2), lane + zdx);
+                    const T vg = MPM ? T(0) : __shfl_sync(FULL, pick_row(gdy, gin4, gin3, gin2), lane + gdx);
+                    if (flags & 1u) hbh = vh;
+                    if (flags & 2u) {
+                        if (flags & 4u) { hbu = m0; hbv = m1; }
+                        else { hbu = m0 * vu + m1 * vv; hbv = m2c * vu + m3 * vv; }
+                    }
+                    if (flags & 8u) zb1 = vz;
+                    if (!MPM && (flags & 16u)) gb1 = vg;
+                }
+            }
+
+            // ================= E: grass factor, Exner cell and faces of row q
+            const bool mq = HAS_MASK && ((mwin >> 2) & 1u);
+            const bool mq1 = HAS_MASK && ((mwin >> 3) & 1u);
+            const T Gq = MPM ? mpm_grass(hbh, hbu, hbv, mq, a.sed) : const_grass(hbh, gb1, mq);
+            const ECell<T> e3 = make_ecell(hbh, hbu, hbv, zb1, Gq);
+            T xe3 = 0;
+            {
+                const ECell<T> ee = shfl_down_ecell(e3);
+                const bool mqe = HAS_MASK ? (__shfl_down_sync(FULL, (int)mq, 1) != 0) : false;
+                const bool xact = rowD && has_e && exner_active(e3, ee, mq, mqe);
+                const T F = xact ? exner_face<T, false>(e3, ee) : T(0);
+                const T Fw = __shfl_up_sync(FULL, F, 1);
+                const bool wact = (__shfl_up_sync(FULL, (int)xact, 1) != 0) && lane > 0;
+                // roe_exner.py:710-711: -F of the west face first, then +F of the east face
+                if (wact) xe3 = xe3 + (-Fw);
+                if (xact) xe3 = xe3 + F;
+            }
+            const bool yex = rowD && (q - 1 >= L0) && colok && exner_active(e4, e3, mq1, mq);
+            const T Fy = yex ? exner_face<T, true>(e4, e3) : T(0);
+
+            // ================= F: z_b update of row r-4
+            T zbp4 = 0;
+            if (r - 4 >= L0 && r - 4 < L1) {
+                T acc = xe4;
+                acc = acc + (-fn4);  // north face (roe_exner.py:712)
+                acc = acc + Fy;      // south face (roe_exner.py:713)
+                zbp4 = e4.zb - dt * acc / dx;
+            }
+            const T gg4 = e4.G;
+
+            // ================= G: second boundary application and stores of row p = r-5
+            const int p = r - 5;
+            const bool rowG = (p >= L0) && (p < L1);
+            T zfin = zbp5, gfin = gg5;
+            if (a.ring != nullptr && rowG) {
+                const int slot = colok ? ring_slot(p, c, ny, nx) : -1;
+                unsigned flags = 0;
+                int zdy = 0, zdx = 0, gdy = 0, gdx = 0;
+                if (slot >= 0) {
+                    const pxb_ring_recipe& rc = a.ring[slot];
+                    flags = rc.flags;
+                    zdy = rc.zb_dy; zdx = rc.zb_dx; gdy = rc.g_dy; gdx = rc.g_dx;
+                }
+                if (__any_sync(FULL, (flags & 24u) != 0)) {
+                    const T vz = __shfl_sync(FULL, pick_row(zdy, zbp6, zbp5, zbp4), lane + zdx);
+                    const T vg = __shfl_sync(FULL, pick_row(gdy, gg6, gg5, gg4), lane + gdx);
+                    if (flags & 8u) zfin = vz;
+                    if (flags & 16u) gfin = vg;
+                }
+            }
+            if (rowG && p >= R0 && p < R1 && out_col) {
+                const long long i = (long long)p * pitch + c;
+                if (AVG) {
+                    zfin = T(0.5) * a.azb[i] + T(0.5) * zfin;
+                    if (a.oG) gfin = T(0.5) * a.aG[i] + T(0.5) * gfin;
+                }
+                a.ozb[i] = zfin;
+                if (a.oG) a.oG[i] = gfin;
+                bad |= !d_isfinite(zfin);
+            }
+            if (rowD && q >= R0 && q < R1 && out_col) {
+                const long long i = (long long)q * pitch + c;
+                T oh = hbh, ou = hbu, ov = hbv;
+                if (AVG) {
+                    oh = T(0.5) * a.ah[i] + T(0.5) * oh;
+                    ou = T(0.5) * a.ahu[i] + T(0.5) * ou;
+                    ov = T(0.5) * a.ahv[i] + T(0.5) * ov;
+                }
+                a.oh[i] = oh;
+                a.ohu[i] = ou;
+                a.ohv[i] = ov;
+                bad |= !(d_isfinite(oh) && d_isfinite(ou) && d_isfinite(ov));
+            }
+
+            // ================= shift the windows
+            pA = pr; hA = h_r; huA = hu_r; hvA = hv_r;
+            xfA0 = xf0; xfA1 = xf1; xfA2 = xf2;
+            nfA0 = yP[0]; nfA1 = yP[1]; nfA2 = yP[2];
+            zt3 = zt2; zt2 = ztA; ztA = zt_r;
+            hr3 = hr2; hr2 = hr1; hur2 = hur1; hvr2 = hvr1;
+            mwin = (mwin << 1) | (m_r ? 1u : 0u);
+            zin4 = zin3; zin3 = zin2; zin2 = zin1; zin1 = zb_r;
+            if (!MPM) { gin4 = gin3; gin3 = gin2; gin2 = gin1; gin1 = g_r; }
+            hf4h = hf3h; hf4u = hf3u; hf4v = hf3v;
+            hf3h = hf2h; hf3u = hf2u; hf3v = hf2v;
+            e4 = e3; xe4 = xe3; fn4 = Fy;
+            zbp6 = zbp5; zbp5 = zbp4;
+            gg6 = gg5; gg5 = gg4;
+        }
+    }
+    if (bad) atomicOr(a.err, 1);
+}
+
+}  // namespace pxb

@@ -1,0 +1,164 @@
+"""Integrator bundles behind PyExner's registry (src/PyExner/integrators/registry.py).
+
+"Forward Euler" follows src/PyExner/integrators/forwardeuler.py:32-132 and "SSPRK2" the
+intended form of src/PyExner/integrators/SSPRK2.py:30-51 (dt from u^n, two stages at the
+same time argument, 0.5*u^n + 0.5*u^(2) on every leaf).
+
+Two ways to run:
+  * ``run_steps`` - a fixed number of steps, entirely on the device: the step (CFL
+    reduction + stages) is captured once into a CUDA graph and replayed; dt never
+    leaves the GPU (``pxb_re_run`` / ``pxb_roe_run``).  This is the timed hot path.
+  * ``run_fn``    - the reference's time-driven loop with output windows.  Deciding
+    when a window ends needs dt on the host, so this path synchronises once per step;
+    it serves the YAML driver, not the benchmark.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Callable, NamedTuple
+
+import torch
+
+from . import _lib
+from .solvers import _re_plan, _roe_plan, _stream
+from .state import RoeExnerState, alloc_plane
+
+TIMESTEP_TOL = 5e-7  # src/utils/constants.py:25
+
+
+class IntegratorConfig(NamedTuple):
+    cfl: float
+    end_time: float
+    out_freq: float
+    solver_config: object
+    solver_bundle: object
+    n_steps: int = None
+
+
+class IntegratorBundle(NamedTuple):
+    name: str
+    config: Callable
+    run_fn: Callable
+
+
+INTEGRATOR_REGISTRY: dict = {}
+
+
+def register_integrator_bundle(name):
+    def decorator(bundle):
+        INTEGRATOR_REGISTRY[name] = bundle()
+        return bundle()
+
+    return decorator
+
+
+def create_integrator_bundle(name):
+    bundle = INTEGRATOR_REGISTRY.get(name)
+    if bundle is None:
+        raise ValueError(f"Unknown integration scheme '{name}'. Available options: {list(INTEGRATOR_REGISTRY.keys())}")
+    return bundle
+
+
+def _config(cfl, end_time, out_freq, solver_bundle, solver_config, n_steps=None):
+    return IntegratorConfig(cfl=cfl, end_time=end_time, out_freq=out_freq, solver_config=solver_config,
+                            solver_bundle=solver_bundle, n_steps=n_steps)
+
+
+def scratch_like(state):
+    ny, nx = state.shape
+    kw = {}
+    for f in state.PLANES:
+        kw[f] = alloc_plane(ny, nx, state.dtype, state.h.device)
+    if isinstance(state, RoeExnerState):
+        kw["seds"] = state.seds
+    return type(state)(**kw)
+
+
+def run_steps(state, mask, solver_config, scheme, n_steps, cfl, scratch=None, log_dt=True):
+    """Advance ``state`` IN PLACE by ``n_steps`` steps on the device.
+
+    Returns the device tensor of the dts taken (or None).  ``scratch`` is a second
+    state of the same layout (allocated when not given)."""
+    code = _lib.SSPRK2 if scheme == "SSPRK2" else _lib.FE
+    b = scratch if scratch is not None else scratch_like(state)
+    dts = torch.empty(max(1, n_steps), dtype=state.dtype, device=state.h.device) if log_dt else None
+    dptr = ctypes.c_void_p(dts.data_ptr()) if dts is not None else None
+    if isinstance(state, RoeExnerState):
+        plan = _re_plan(state, mask, solver_config)
+        _lib.call("pxb_re_run", plan.handle, ctypes.byref(state.c_fields()), ctypes.byref(b.c_fields()),
+                  int(n_steps), code, float(cfl), dptr, _stream())
+    else:
+        plan = _roe_plan(state, solver_config)
+        _lib.call("pxb_roe_run", plan.handle, ctypes.byref(state.c_fields()), ctypes.byref(b.c_fields()),
+                  int(n_steps), code, float(cfl), dptr, _stream())
+    return dts[:n_steps] if dts is not None else None
+
+
+def check_state(state, mask, solver_config):
+    """Raise if a kernel flagged a non-finite dt or state value since the last check."""
+    if isinstance(state, RoeExnerState):
+        _re_plan(state, mask, solver_config).check()
+    else:
+        _roe_plan(state, solver_config).check()
+
+
+def _ssprk2_step(bundle, st, t, dt, mask, cfg):
+    s1 = bundle.step_fn(st, t, dt, mask, cfg)
+    return bundle.step_fn(s1, t, dt, mask, cfg, avg=st)
+
+
+def _run_time_loop(state, config, io, mesh, b_mask, ssprk2):
+    bundle = config.solver_bundle
+    cfg = config.solver_config
+    mask = bundle.mask_fn(state, cfg.mpi_handler, b_mask)
+    state = bundle.init_fn(state, mask, cfg)
+    if config.n_steps is not None:
+        run_steps(state, mask, cfg, "SSPRK2" if ssprk2 else "FE", config.n_steps, config.cfl)
+        check_state(state, mask, cfg)
+        return state
+    if io is not None:
+        io.write_state(state, mesh, mask[0])
+    time = 0.0
+    num_out = 0
+    while time < config.end_time - TIMESTEP_TOL:
+        dt = float(bundle.compute_dt_fn(state, config.cfl, mask, cfg))
+        next_out = (int(time / config.out_freq) + 1) * config.out_freq
+        target = min(next_out, config.end_time)
+        if time + dt >= target - TIMESTEP_TOL:
+            if ssprk2:
+                # SSPRK2.py:222-225: the last step of a window lands on the target
+                dt = target - time
+            else:
+                # forwardeuler.py:93-109: probe step to the target for output only
+                probe = bundle.step_fn(state, time, target - time, mask, cfg)
+                if io is not None:
+                    io.write_state(probe, mesh, mask[0])
+                num_out += 1
+        if ssprk2:
+            state = _ssprk2_step(bundle, state, time, dt, mask, cfg)
+            if io is not None and abs((time + dt) - target) < TIMESTEP_TOL:
+                io.write_state(state, mesh, mask[0])
+                num_out += 1
+        else:
+            state = bundle.step_fn(state, time, dt, mask, cfg)
+        time += dt
+    check_state(state, mask, cfg)
+    return state
+
+
+def run_fn_forwardeuler(state, config, io=None, mesh=None, b_mask=None):
+    return _run_time_loop(state, config, io, mesh, b_mask, ssprk2=False)
+
+
+def run_fn_ssprk2(state, config, io=None, mesh=None, b_mask=None):
+    return _run_time_loop(state, config, io, mesh, b_mask, ssprk2=True)
+
+
+@register_integrator_bundle("Forward Euler")
+def integrator_forwardeuler():
+    return IntegratorBundle(name="Forward Euler", config=_config, run_fn=run_fn_forwardeuler)
+
+
+@register_integrator_bundle("SSPRK2")
+def integrator_ssprk2():
+    return IntegratorBundle(name="SSPRK2", config=_config, run_fn=run_fn_ssprk2)

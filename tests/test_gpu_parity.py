@@ -1,0 +1,209 @@
+"""Parity of the CUDA path with the oracle (GPU only).
+
+Float64 builds follow the reference's operation order; per-stage results must agree
+with the oracle to 1e-12 normwise relative error (max|gpu - oracle| / max|oracle| per
+plane), and to 1e-10 after six steps (rounding of the transcendental functions grows
+slowly through the wave-speed switches).  Float32 results are held to 2e-5 normwise
+per stage and 1e-4 after six steps.
+"""
+import numpy as np
+import pytest
+import torch
+
+from helpers import (CASES, RE_PLANES, ROE_BC_SPECS, ROE_CASES, golden_re, grid_coords, l1_rel, oracle_setup,
+                     random_re_case, rel_err)
+from oracle import boundaries as OB
+from oracle import integrators as OI
+from oracle import roe as OR
+from oracle import roe_exner as ORE
+
+pytestmark = pytest.mark.gpu
+
+TOL = {torch.float64: (1e-12, 1e-10), torch.float32: (2e-5, 1e-4)}
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _lib_built():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from pyexner_b200 import build
+
+    build.build()
+
+
+def device_re(arrs, params, X, Y, seds, dtype, dx):
+    from pyexner_b200 import BoundaryManager, RoeExnerState, create_solver_bundle
+
+    bm = BoundaryManager(params, X, Y)
+    st = RoeExnerState.from_numpy(arrs, seds, dtype)
+    bundle = create_solver_bundle("Roe Exner")
+    cfg = bundle.config(st, None, bm, dx, params)
+    mask = bundle.mask_fn(st, None, bm.boundary_mask)
+    st = bundle.init_fn(st, mask, cfg)
+    return bundle, cfg, mask, st
+
+
+def assert_planes(got, ref, tol, planes=RE_PLANES, what=""):
+    for f in planes:
+        e = rel_err(got[f], ref[f])
+        assert e <= tol, f"{what} {f}: normwise relative error {e:.3e} > {tol:.1e}"
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "f32"])
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_roe_exner_golden(request, case, dtype):
+    from pyexner_b200 import run_steps
+    from pyexner_b200.integrators import check_state
+
+    d, arrs, params, X, Y, mpm = golden_re(request.config.rootpath, case)
+    dx = float(d["dx"])
+    tol1, tolN = TOL[dtype]
+    bundle, cfg, mask, st = device_re(arrs, params, X, Y, d["seds"], dtype, dx)
+    assert np.array_equal(mask.cpu().numpy(), d["mask"])
+    init = st.to_numpy()
+    assert_planes(init, {f: d[f"init_{f}"] for f in RE_PLANES}, tol1, what="init")
+    dt = bundle.compute_dt_fn(st, 0.5, mask, cfg)
+    assert rel_err(float(dt), float(d["dt0"])) <= tol1
+    # one stage with the reference's dt
+    s1 = bundle.step_fn(st, 0.0, float(d["dt0"]), mask, cfg)
+    assert_planes(s1.to_numpy(), {f: d[f"stage1_{f}"] for f in RE_PLANES}, tol1, what="stage")
+    for scheme, tag in (("FE", "fe"), ("SSPRK2", "rk")):
+        s = st.clone()
+        dts = run_steps(s, mask, cfg, scheme, 6, 0.5)
+        check_state(s, mask, cfg)
+        assert rel_err(dts.cpu().numpy(), d[f"{tag}_dts"]) <= tolN
+        assert_planes(s.to_numpy(), {f: d[f"{tag}_{f}"] for f in RE_PLANES}, tolN, what=scheme)
+
+
+@pytest.mark.parametrize("shape,band_rows,regime,bc,mpm", [
+    ((70, 100), 8, "fast", "trans_x_refl_y", True),
+    ((131, 61), 16, "wetdry", "refl_all", True),
+    ((57, 83), 9, "fast", "influx_left", False),
+    ((64, 55), 7, "wetdry", "partial_nodata", False),
+    ((40, 29), 5, "fast", "refl_first", True),
+    ((37, 30), 6, "smooth", "trans_x_refl_y", True),
+])
+def test_roe_exner_strips_and_bands(shape, band_rows, regime, bc, mpm):
+    """Grids spanning several warp strips and row bands, checked against the oracle."""
+    from pyexner_b200 import run_steps
+    from pyexner_b200.cases import seds_matrix
+
+    ny, nx = shape
+    arrs, params, X, Y, mpm = random_re_case(ny, nx, seed=ny * 1000 + nx, regime=regime, bcname=bc, mpm=mpm)
+    params["band_rows"] = band_rows
+    seds = seds_matrix(params["erosion"])
+    dx = 0.1
+    ost, omask, obcs = oracle_setup(arrs, params, X, Y, mpm, seds)
+    odt = ORE.compute_dt(ost, 0.5, dx, omask[0])
+    o1 = ORE.stage(ost, odt, dx, omask, obcs, mpm)
+    orun, odts = OI.run_roe_exner(ost, omask, obcs, mpm, dx, 0.5, 4, "SSPRK2")
+    bundle, cfg, mask, st = device_re(arrs, params, X, Y, seds, torch.float64, dx)
+    assert_planes(st.to_numpy(), ost, 1e-12, what="init")
+    s1 = bundle.step_fn(st, 0.0, float(odt), mask, cfg)
+    assert_planes(s1.to_numpy(), o1, 1e-12, what="stage")
+    s = st.clone()
+    dts = run_steps(s, mask, cfg, "SSPRK2", 4, 0.5)
+    assert rel_err(dts.cpu().numpy(), odts) <= 1e-10
+    assert_planes(s.to_numpy(), orun, 1e-10, what="ssprk2")
+
+
+def test_ssprk2_stage_api_matches_run_loop():
+    """step_fn twice with the average equals one device SSPRK2 step."""
+    from pyexner_b200 import run_steps
+    from pyexner_b200.cases import seds_matrix
+
+    arrs, params, X, Y, mpm = random_re_case(45, 52, seed=5, regime="fast")
+    seds = seds_matrix(params["erosion"])
+    bundle, cfg, mask, st = device_re(arrs, params, X, Y, seds, torch.float64, 0.1)
+    dt = bundle.compute_dt_fn(st, 0.5, mask, cfg)
+    s1 = bundle.step_fn(st, 0.0, dt, mask, cfg)
+    s2 = bundle.step_fn(s1, 0.0, dt, mask, cfg, avg=st)
+    s = st.clone()
+    run_steps(s, mask, cfg, "SSPRK2", 1, 0.5)
+    got, ref = s.to_numpy(), s2.to_numpy()
+    for f in ("h", "hu", "hv", "z_b", "G"):
+        assert np.array_equal(got[f], ref[f]), f
+
+
+def device_roe(arrs, spec, X, Y, dtype, dx):
+    from pyexner_b200 import BoundaryManager, RoeState, create_solver_bundle
+
+    params = dict(flux_scheme="Roe", boundaries=spec)
+    bm = BoundaryManager(params, X, Y)
+    st = RoeState.from_numpy(arrs, dtype)
+    bundle = create_solver_bundle("Roe")
+    cfg = bundle.config(st, None, bm, dx, params)
+    mask = bundle.mask_fn(st)
+    st = bundle.init_fn(st, mask, cfg)
+    return bundle, cfg, mask, st
+
+
+@pytest.mark.parametrize("case", ROE_CASES, ids=[c[0] for c in ROE_CASES])
+def test_roe_golden(request, case):
+    from pyexner_b200 import run_steps
+
+    name, (ny, nx), _regime, bcname = case
+    d = np.load(request.config.rootpath / "tests" / "golden" / f"roe_{name}.npz")
+    X, Y = grid_coords(ny, nx)
+    arrs = {f: d[f"in_{f}"] for f in ("h", "hu", "hv", "z", "n")}
+    dx = float(d["dx"])
+    bundle, cfg, mask, st = device_roe(arrs, ROE_BC_SPECS[bcname](ny, nx), X, Y, torch.float64, dx)
+    dt = bundle.compute_dt_fn(st, 0.5, mask, cfg)
+    assert rel_err(float(dt), float(d["dt0"])) <= 1e-12
+    s1 = bundle.step_fn(st, 0.0, float(d["dt0"]), mask, cfg)
+    assert_planes(s1.to_numpy(), {f: d[f"stage1_{f}"] for f in ("h", "hu", "hv", "z", "n")}, 1e-12,
+                  planes=("h", "hu", "hv", "z", "n"), what="stage")
+    s = st.clone()
+    dts = run_steps(s, mask, cfg, "SSPRK2", 6, 0.5)
+    assert rel_err(dts.cpu().numpy(), d["rk_dts"]) <= 1e-10
+    assert_planes(s.to_numpy(), {f: d[f"rk_{f}"] for f in ("h", "hu", "hv", "z", "n")}, 1e-10,
+                  planes=("h", "hu", "hv", "z", "n"), what="ssprk2")
+
+
+def test_roe_dambreak_200_steps():
+    """The plain Roe dam-break (256^2, float64, SSPRK2, 200 steps) against the oracle."""
+    from pyexner_b200 import cases, run_steps
+
+    c = cases.dambreak_roe(256)
+    ny, nx = c["arrs"]["h"].shape
+    spec = c["params"]["boundaries"]
+    bundle, cfg, mask, st = device_roe(c["arrs"], spec, c["X"], c["Y"], torch.float64, c["dx"])
+    dts = run_steps(st, mask, cfg, "SSPRK2", 200, 0.5)
+    obcs = OB.Boundaries("Roe", spec, c["X"], c["Y"])
+    ost, odts = OI.run_roe({k: np.array(v) for k, v in c["arrs"].items()}, obcs, c["dx"], 0.5, 200, "SSPRK2")
+    assert rel_err(dts.cpu().numpy(), odts) <= 1e-9
+    got = st.to_numpy()
+    for f in ("h", "hu", "hv"):
+        assert rel_err(got[f], ost[f]) <= 1e-9, f
+        assert l1_rel(got[f], ost[f]) <= 1e-10, f
+
+
+def test_nonfinite_state_is_reported():
+    from pyexner_b200 import run_steps
+    from pyexner_b200._lib import ERR_NONFINITE, PxbError
+    from pyexner_b200.cases import seds_matrix
+    from pyexner_b200.integrators import check_state
+
+    arrs, params, X, Y, mpm = random_re_case(30, 40, seed=9)
+    arrs["hu"][10, 10] = np.nan
+    seds = seds_matrix(params["erosion"])
+    bundle, cfg, mask, st = device_re(arrs, params, X, Y, seds, torch.float32, 0.1)
+    run_steps(st, mask, cfg, "SSPRK2", 2, 0.5)
+    with pytest.raises(PxbError) as e:
+        check_state(st, mask, cfg)
+    assert e.value.code == ERR_NONFINITE
+    check_state(st, mask, cfg)  # the flag was cleared by the first check
+
+
+def test_unreachable_boundary_layout_is_rejected():
+    from pyexner_b200._lib import ERR_UNSUPPORTED, PxbError
+    from pyexner_b200.cases import seds_matrix
+
+    arrs, params, X, Y, mpm = random_re_case(20, 24, seed=3)
+    # a boundary polygon around an interior cell: the stage kernels handle ring cells only
+    params["boundaries"]["inner"] = {"type": "Transmissive", "polygon": [[9.5, 9.5], [10.5, 9.5], [10.5, 10.5],
+                                                                          [9.5, 10.5]],
+                                     "values": [0, 0, 0, 0], "normal": [1.0, 0.0]}
+    with pytest.raises(PxbError) as e:
+        device_re(arrs, params, X, Y, seds_matrix(params["erosion"]), torch.float64, 0.1)
+    assert e.value.code == ERR_UNSUPPORTED
