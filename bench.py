@@ -291,6 +291,20 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def profile_sequence(args):
+    import torch
+
+    from pyexner_b200 import build, run_steps
+    from pyexner_b200.integrators import check_state
+
+    build.build()
+    dt = torch.float32 if args.dtype == "f32" else torch.float64
+    c, bundle, cfg, mask, st = build_case(args.n, dt, "cuda")
+    run_steps(st, mask, cfg, "SSPRK2", max(1, args.warmup), 0.5)
+    torch.cuda.synchronize()
+    check_state(st, mask, cfg)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -300,9 +314,14 @@ def main():
     ap.add_argument("--impl", default="b200")
     ap.add_argument("--accuracy-steps", type=int, default=2000)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="short fixed sequence for ncu: build the case, run --warmup SSPRK2 steps, exit")
+    ap.add_argument("--dtype", default="f32", choices=["f32", "f64"])
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.profile:
+        return profile_sequence(args)
 
     import torch
     import torch.distributed as dist

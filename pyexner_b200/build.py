@@ -56,9 +56,10 @@ def build(force=False, verbose=False):
         return LIB
     os.makedirs(BUILD, exist_ok=True)
     objs = []
+    knobs = os.environ.get("PXB_NVCC_DEFINES", "").split()  # e.g. "-DPXB_ROW_UNROLL=2" for tuning sweeps
     for src, extra in UNITS:
         obj = os.path.join(BUILD, src.replace(".cu", ".o"))
-        cmd = [nvcc(), *ARCH, *COMMON, *extra, "-c", os.path.join(CSRC, src), "-o", obj]
+        cmd = [nvcc(), *ARCH, *COMMON, *extra, *knobs, "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

@@ -312,7 +312,15 @@ void fill_sed(pxb::SedTable<T>& S, const double* seds, int nsed) {
         d50f_sum += d50 * frac;
     }
     S.one_minus_por = (T)(1.0 - por_sum / nsed);
+    S.inv_one_minus_por = (T)(1.0 / (1.0 - por_sum / nsed));
     S.n_p_mix = (T)(std::pow(d50f_sum / nsed, 1.0 / 6.0) / 21.1);
+    for (int k = 0; k < nsed; ++k) {
+        const double frac = seds[0 * nsed + k], d50 = seds[1 * nsed + k], dens = seds[2 * nsed + k];
+        const double s = dens / 1000.0;
+        const double np_ = std::pow(d50, 1.0 / 6.0) / 21.1;
+        S.k_theta[k] = (T)(np_ * np_ / ((s - 1.0) * d50));
+        S.k_g1[k] = (T)(8.0 * frac * std::pow(np_, 3.0) * std::sqrt(9.81) / (s - 1.0));
+    }
 }
 
 struct PlanCommon {

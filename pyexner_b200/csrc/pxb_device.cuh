@@ -44,6 +44,21 @@ __device__ __forceinline__ double d_cos(double x) { return cos(x); }
 __device__ __forceinline__ bool d_isfinite(float x) { return isfinite(x); }
 __device__ __forceinline__ bool d_isfinite(double x) { return isfinite(x); }
 
+// Float32 building blocks.  The float build trades the last ulp for throughput: the
+// hardware approximations below are accurate to about 2^-22 relative, far inside the
+// float32 accuracy budget of the step.  The float64 build uses none of them.
+__device__ __forceinline__ float f_rcp(float x) { float y; asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x)); return y; }
+__device__ __forceinline__ float f_rsqrt(float x) { float y; asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x)); return y; }
+__device__ __forceinline__ float f_sqrt(float x) { float y; asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x)); return y; }
+__device__ __forceinline__ float f_lg2(float x) { float y; asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x)); return y; }
+__device__ __forceinline__ float f_ex2(float x) { float y; asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x)); return y; }
+// Products that must not be fused into an FMA: sign decisions of the Exner upwinding
+// depend on exact cancellations (mirror states at reflective walls give exactly 0).
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+template <class T>
+__host__ __device__ constexpr bool is_f32() { return sizeof(T) == 4; }
+
 // ---------------------------------------------------------------- hydrodynamic faces
 // Per-cell values used by the Roe-Exner face flux (roe_exner.py:317-335, 421-425, 455).
 template <class T>
@@ -63,10 +78,19 @@ __device__ __forceinline__ HCell<T> make_hcell(T h, T hu, T hv, T zb, T z, T nb)
     const T hc = clamp_lo(h, T(DRY_TOL));
     const bool wet = hc > T(DRY_TOL);
     p.h = hc;
-    p.u = wet ? hu / hc : T(0);
-    p.v = wet ? hv / hc : T(0);
-    p.sq = d_sqrt(hc);
-    p.c = d_sqrt(T(G_ACC) * hc);
+    if constexpr (is_f32<T>()) {
+        const float rs = f_rsqrt(hc);
+        const float r = rs * rs;
+        p.u = wet ? hu * r : 0.f;
+        p.v = wet ? hv * r : 0.f;
+        p.sq = hc * rs;
+        p.c = 3.1320919526731650f * p.sq;  // sqrt(g) sqrt(h)
+    } else {
+        p.u = wet ? hu / hc : T(0);
+        p.v = wet ? hv / hc : T(0);
+        p.sq = d_sqrt(hc);
+        p.c = d_sqrt(T(G_ACC) * hc);
+    }
     const T zbc = zb > T(SED_TOL) ? zb : T(SED_TOL * 0.01);
     p.zt = z + zbc;
     p.nb = nb;
@@ -82,9 +106,19 @@ __device__ __forceinline__ void roe_exner_face(const HCell<T>& I, const HCell<T>
     const T uhj = YF ? -J.v : J.u, vhj = YF ? J.u : J.v;
     const T den = I.sq + J.sq;
     const T ht = T(0.5) * (I.h + J.h);
-    const T ct = d_sqrt(T(G_ACC) * ht);
-    const T ut = (uhi * I.sq + uhj * J.sq) / den;
-    const T vt = (vhi * I.sq + vhj * J.sq) / den;
+    T ct, ut, vt, rct = T(0);
+    if constexpr (is_f32<T>()) {
+        const float rden = f_rcp(den);
+        const float gh = 9.81f * ht;
+        rct = f_rsqrt(gh);
+        ct = gh * rct;
+        ut = (uhi * I.sq + uhj * J.sq) * rden;
+        vt = (vhi * I.sq + vhj * J.sq) * rden;
+    } else {
+        ct = d_sqrt(T(G_ACC) * ht);
+        ut = (uhi * I.sq + uhj * J.sq) / den;
+        vt = (vhi * I.sq + vhj * J.sq) / den;
+    }
     const T l1r = ut - ct;
     const T l3r = ut + ct;
     // Harten-Hyman (roe_exner.py:357-371); the VEL_TOL guard only in the lambda_3 speed
@@ -107,19 +141,50 @@ __device__ __forceinline__ void roe_exner_face(const HCell<T>& I, const HCell<T>
     const T dh = J.h - I.h;
     const T dhu = J.h * uhj - I.h * uhi;
     const T dhv = J.h * vhj - I.h * vhi;
-    const T den2 = T(-2.0) * ct;
-    const T a1 = (-l3r * dh + dhu) / den2;
-    const T a2 = (-vt * dh + dhv) / ct;
-    const T a3 = (l1r * dh - dhu) / den2;
     const T dz = J.zt - I.zt;
     const T thrust = -T(G_ACC) * ht * dz;
     const T nt = T(0.5) * (I.nb + J.nb);
-    const T sf = (nt * nt * d_sqrt(ut * ut + vt * vt) * ut) / clamp_lo(d_pow(ht, T(4.0 / 3.0)), T(DRY_TOL));
-    const T tau = T(G_ACC) * ht * sf * dx;
-    const T b1 = (thrust - tau) / den2;
+    T a1, a2, a3, b1;
+    if constexpr (is_f32<T>()) {
+        const float r2 = -0.5f * rct;  // 1 / (-2 c)
+        a1 = (-l3r * dh + dhu) * r2;
+        a2 = (-vt * dh + dhv) * rct;
+        a3 = (l1r * dh - dhu) * r2;
+        // h^(-4/3) with the DRY_TOL floor of h^(4/3) (h^(4/3) < DRY_TOL  <=>  h < DRY_TOL^(3/4))
+        const float rp = ht < 1e-3f ? 1e4f : f_ex2(-1.3333333333f * f_lg2(ht));
+        const float sf = nt * nt * f_sqrt(ut * ut + vt * vt) * ut * rp;
+        const float tau = 9.81f * ht * sf * dx;
+        b1 = (thrust - tau) * r2;
+    } else {
+        const T den2 = T(-2.0) * ct;
+        a1 = (-l3r * dh + dhu) / den2;
+        a2 = (-vt * dh + dhv) / ct;
+        a3 = (l1r * dh - dhu) / den2;
+        const T sf = (nt * nt * d_sqrt(ut * ut + vt * vt) * ut) / clamp_lo(d_pow(ht, T(4.0 / 3.0)), T(DRY_TOL));
+        const T tau = T(G_ACC) * ht * sf * dx;
+        b1 = (thrust - tau) / den2;
+    }
     const T b3 = -b1;
     // Upwinded waves (roe_exner.py:484-507); P columns (1,l1,vt), (0,0,ct), (1,l3,vt).
     T p0 = T(0), p1 = T(0), p2 = T(0), n0 = T(0), n1 = T(0), n2 = T(0);
+    if constexpr (is_f32<T>()) {
+        // branch-free: each wave goes to one side by its speed's sign (NaN speeds to none)
+        const float w1 = l1 * a1 - b1, w2 = ut * a2, w3 = l3 * a3 - b3;
+        const float e1 = m1 ? lE1 * a1 : 0.f, e3 = m3 ? lE3 * a3 : 0.f;
+        const bool s1 = l1 > 0.f, s2 = ut > 0.f, s3 = l3 > 0.f, t1 = lE1 > 0.f, t3 = lE3 > 0.f;
+        const bool z1 = l1 <= 0.f, z2 = ut <= 0.f, z3 = l3 <= 0.f;
+        const float q0a = s1 ? w1 : 0.f, q0b = s3 ? w3 : 0.f;
+        const float r0a = z1 ? w1 : 0.f, r0b = z3 ? w3 : 0.f;
+        const float ep1 = t1 ? e1 : 0.f, en1 = t1 ? 0.f : e1;
+        const float ep3 = t3 ? e3 : 0.f, en3 = t3 ? 0.f : e3;
+        p0 = q0a + q0b + ep1 + ep3;
+        n0 = r0a + r0b + en1 + en3;
+        p1 = q0a * l1 + q0b * l3 + ep1 * l1 + ep3 * l3;
+        n1 = r0a * l1 + r0b * l3 + en1 * l1 + en3 * l3;
+        const float wc = w2 * ct;
+        p2 = (q0a + q0b + ep1 + ep3) * vt + (s2 ? wc : 0.f);
+        n2 = (r0a + r0b + en1 + en3) * vt + (z2 ? wc : 0.f);
+    } else {
     {
         const T w = l1 * a1 - b1;
         if (l1 > T(0)) { p0 = p0 + w; p1 = p1 + w * l1; p2 = p2 + w * vt; }
@@ -145,6 +210,7 @@ __device__ __forceinline__ void roe_exner_face(const HCell<T>& I, const HCell<T>
         const T e = lE3 * a3;
         if (lE3 > T(0)) { p0 = p0 + e; p1 = p1 + e * l3; p2 = p2 + e * vt; }
         else if (lE3 <= T(0)) { n0 = n0 + e; n1 = n1 + e * l3; n2 = n2 + e * vt; }
+    }
     }
     // back to (x, y) (roe_exner.py:526-531)
     if (YF) {
@@ -176,9 +242,17 @@ __device__ __forceinline__ ECell<T> make_ecell(T h, T hu, T hv, T zb, T G) {
     e.h = h;
     e.zb = zb;
     e.zbe = zb > T(SED_TOL) ? zb : T(SED_TOL * 0.01);
-    e.sq = d_sqrt(he);
-    e.u = wet ? hu / he : T(0);
-    e.v = wet ? hv / he : T(0);
+    if constexpr (is_f32<T>()) {
+        const float rs = f_rsqrt(he);
+        const float r = rs * rs;
+        e.sq = he * rs;
+        e.u = wet ? hu * r : 0.f;
+        e.v = wet ? hv * r : 0.f;
+    } else {
+        e.sq = d_sqrt(he);
+        e.u = wet ? hu / he : T(0);
+        e.v = wet ? hv / he : T(0);
+    }
     e.um = e.u * e.u + e.v * e.v;
     e.G = G;
     return e;
@@ -188,16 +262,32 @@ template <class T, bool YF>
 __device__ __forceinline__ T exner_face(const ECell<T>& I, const ECell<T>& J) {
     const T uhi = YF ? -I.v : I.u;
     const T uhj = YF ? -J.v : J.u;
-    const T ut = (uhi * I.sq + uhj * J.sq) / (I.sq + J.sq);
     const T qi = I.G * I.um * uhi;
     const T qj = J.G * J.um * uhj;
     const T gt = T(0.5) * (I.G + J.G);
     const T dz = J.zbe - I.zbe;
-    const T dq = gt * J.um * uhj - gt * I.um * uhi;
-    const T lam4 = fabs(dz) > T(SED_TOL) ? dq / dz : ut;
     const T qbi = qi + (gt - I.G) * I.um * uhi;
     const T qbj = qj + (gt - J.G) * J.um * uhj;
-    return lam4 >= T(0) ? qbi : qbj;
+    // lambda_4 = dq/dz, or the Roe-averaged normal velocity when |dz| <= SED_TOL; only
+    // its sign is used.  Products are rounded separately (no FMA) so that exact
+    // cancellations stay exact, as in the reference's arithmetic.
+    const bool big = fabs(dz) > T(SED_TOL);
+    bool up;
+    if constexpr (is_f32<T>()) {
+        if (big) {
+            const float dq = mul_rn(mul_rn(gt, J.um), uhj) - mul_rn(mul_rn(gt, I.um), uhi);
+            up = (dq == 0.f) || (dq == dq && ((dq > 0.f) == (dz > 0.f)));
+        } else {
+            const float num = mul_rn(uhi, I.sq) + mul_rn(uhj, J.sq);  // sign of ut (denominator > 0)
+            up = num >= 0.f;
+        }
+    } else {
+        const T ut = (uhi * I.sq + uhj * J.sq) / (I.sq + J.sq);
+        const T dq = gt * J.um * uhj - gt * I.um * uhi;
+        const T lam4 = big ? dq / dz : ut;
+        up = lam4 >= T(0);
+    }
+    return up ? qbi : qbj;
 }
 
 // Exner face activity (roe_exner.py:687-701): wet on either side, neither side nodata,
@@ -225,11 +315,39 @@ struct SedTable {
     int n;
     T one_minus_por;  // 1 - mean(porosity)
     T n_p_mix;        // (mean(d50*frac))^(1/6) / 21.1   (compute_n)
+    // float path only: folded constants
+    T k_theta[PXB_MAX_SED];  // n_p^2 / ((s-1) d50)
+    T k_g1[PXB_MAX_SED];     // frac * n_p^3 sqrt(g) / (s-1) * 8
+    T inv_one_minus_por;
 };
 
 // Meyer-Peter & Mueller grass factor of one cell (roe_exner.py:85-130).
 template <class T>
 __device__ __forceinline__ T mpm_grass(T h, T hu, T hv, bool nodata, const SedTable<T>& S) {
+    if constexpr (is_f32<T>()) {
+        // G = sum_k frac n_p^3 sqrt(g)/((s-1) sqrt h) * 8 sqrt(dth)/(th^1.5 + 1e-5) * dth
+        const float hc = clamp_lo(h, float(DRY_TOL));
+        // one Newton step each: the threshold (theta - theta_c)^1.5 amplifies errors in theta
+        float rs = f_rsqrt(hc);
+        rs = rs * (1.5f - 0.5f * hc * rs * rs);
+        const float r = rs * rs;
+        const float u = hu * r, v = hv * r;
+        const float vel2 = u * u + v * v;
+        float rcb = f_ex2(-0.33333333333f * f_lg2(hc));  // h^(-1/3)
+        rcb = rcb * (4.f - hc * rcb * rcb * rcb) * (1.f / 3.f);
+        float G = 0.f;
+        for (int k = 0; k < S.n; ++k) {
+            const float th = fmaxf(S.k_theta[k] * vel2 * rcb, 0.f);
+            const float dth = th - S.s[k].thc;
+            if (dth > 0.f) {
+                const float th15 = th * f_sqrt(th);
+                G += S.k_g1[k] * rs * f_sqrt(dth) * dth * f_rcp(th15 + 1e-5f);
+            }
+        }
+        G *= S.inv_one_minus_por;
+        if (nodata) G = 0.f;
+        return hc > float(DRY_TOL) ? G : 0.f;
+    }
     const T hc = clamp_lo(h, T(DRY_TOL));
     const T u = hu / hc, v = hv / hc;
     const T vel2 = u * u + v * v;
@@ -263,15 +381,25 @@ template <class T>
 struct CCell {
     T h;  // max(h, DRY_TOL)
     T sq, u, v, G;
+    T rs;  // 1/sqrt(h) (float path)
 };
 
 template <class T>
 __device__ __forceinline__ CCell<T> make_ccell(T h, T hu, T hv, T G) {
     CCell<T> p;
     p.h = clamp_lo(h, T(DRY_TOL));
-    p.sq = d_sqrt(p.h);
-    p.u = hu / p.h;
-    p.v = hv / p.h;
+    if constexpr (is_f32<T>()) {
+        p.rs = f_rsqrt(p.h);
+        const float r = p.rs * p.rs;
+        p.sq = p.h * p.rs;
+        p.u = hu * r;
+        p.v = hv * r;
+    } else {
+        p.rs = T(0);
+        p.sq = d_sqrt(p.h);
+        p.u = hu / p.h;
+        p.v = hv / p.h;
+    }
     p.G = G;
     return p;
 }
@@ -283,6 +411,33 @@ __device__ __forceinline__ void cubic_extremes(T ut, T at, T ct, T& lmin, T& lma
     if (at < T(1e-5)) {
         lmin = ut - ct;
         lmax = ut + ct;
+        return;
+    }
+    if constexpr (is_f32<T>()) {
+        // float Cardano; where |cos(theta)| is within 1e-3 of 1 (two roots close
+        // together) the trigonometric form loses digits, so those faces redo the
+        // solve in float64.
+        const float b = -2.f * ut;
+        const float c = (1.f + at) * (ct * ct) - ut * ut;
+        const float d = -(ct * ct) * at * ut;
+        const float p = (-3.f * c - b * b) * (1.f / 3.f);
+        const float q = (2.f * b * b * b + 9.f * b * c + 27.f * d) * (-1.f / 27.f);
+        const float xr = (3.f * q) / (2.f * p) * sqrtf(-3.f / p);
+        if (fabsf(xr) > 0.999f || xr != xr) {
+            double dl, du;
+            cubic_extremes<double>(double(ut), double(at), double(ct), dl, du);
+            lmin = float(dl);
+            lmax = float(du);
+            return;
+        }
+        const float th = acosf(xr);
+        const float sq = 2.f * sqrtf(-p * (1.f / 3.f));
+        const float shift = b * (1.f / 3.f);
+        float sn, cs;
+        sincosf(th * (1.f / 3.f), &sn, &cs);
+        lmax = sq * cs + shift;
+        // cos((th + 2 pi)/3) = -cos(th/3)/2 - sqrt(3)/2 sin(th/3)
+        lmin = sq * (-0.5f * cs - 0.86602540378f * sn) + shift;
         return;
     }
     const T b = T(-2) * ut;
@@ -306,10 +461,17 @@ __device__ __forceinline__ T face_speed(const CCell<T>& I, const CCell<T>& J) {
     const T uhj = YF ? -J.v : J.u, vhj = YF ? J.u : J.v;
     const T den = I.sq + J.sq;
     const T ht = T(0.5) * (I.h + J.h);
-    const T ut = (uhi * I.sq + uhj * J.sq) / den;
-    const T ct = d_sqrt(T(G_ACC) * ht);
     const T gt = T(0.5) * (I.G + J.G);
-    const T at = gt * (uhi * uhi + uhi * uhj + uhj * uhj + vhi * vhj) / (I.sq * J.sq);
+    T ut, ct, at;
+    if constexpr (is_f32<T>()) {
+        ut = (uhi * I.sq + uhj * J.sq) * f_rcp(den);
+        ct = f_sqrt(9.81f * ht);
+        at = gt * (uhi * uhi + uhi * uhj + uhj * uhj + vhi * vhj) * (I.rs * J.rs);
+    } else {
+        ut = (uhi * I.sq + uhj * J.sq) / den;
+        ct = d_sqrt(T(G_ACC) * ht);
+        at = gt * (uhi * uhi + uhi * uhj + uhj * uhj + vhi * vhj) / (I.sq * J.sq);
+    }
     const T l1 = ut - ct, l3 = ut + ct;
     T lmin, lmax;
     cubic_extremes(ut, at, ct, lmin, lmax);

@@ -76,6 +76,7 @@ __global__ void __launch_bounds__(256) re_cfl_kernel(const CflArgs<T> a) {
                 e.u = __shfl_down_sync(FULL, cur.u, 1);
                 e.v = __shfl_down_sync(FULL, cur.v, 1);
                 e.G = __shfl_down_sync(FULL, cur.G, 1);
+                e.rs = __shfl_down_sync(FULL, cur.rs, 1);
                 const T he = __shfl_down_sync(FULL, h, 1);
                 const bool me = HAS_MASK ? (__shfl_down_sync(FULL, (int)m, 1) != 0) : false;
                 if (has_e && ((h > DRY) || (he > DRY)) && !(m || me)) {

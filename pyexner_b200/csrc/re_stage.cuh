@@ -21,7 +21,13 @@
 #pragma once
 #include "pxb_device.cuh"
 
+#ifndef PXB_ROW_UNROLL
+#define PXB_ROW_UNROLL 1
+#endif
+
 namespace pxb {
+
+constexpr int kRowUnroll = PXB_ROW_UNROLL;
 
 template <class T>
 struct REStageArgs {
@@ -80,6 +86,7 @@ __global__ void __launch_bounds__(128) re_stage_kernel(const REStageArgs<T> a) {
     const long long pitch = a.pitch;
     const T dt = *a.dt;
     const T dx = a.dx;
+    const T dtdx = dt / dx;  // float path only
     const T DRY = T(DRY_TOL);
     const int nitems = a.nstrips * a.nbands;
     bool bad = false;
@@ -96,6 +103,8 @@ __global__ void __launch_bounds__(128) re_stage_kernel(const REStageArgs<T> a) {
         const int R0 = band * a.band_rows;
         const int R1 = (band == a.nbands - 1) ? ny : R0 + a.band_rows;
         const int L0 = max(0, R0 - 3), L1 = min(ny, R1 + 3);
+        // boundary recipes can only apply in the first/last strip or on rows 0 / ny-1
+        const bool bc_strip = (a.ring != nullptr) && (strip == 0 || last_strip);
 
         // ---- carried pipeline state
         HCell<T> pA = make_hcell(T(0), T(0), T(0), T(0), T(0), T(0));
@@ -110,22 +119,35 @@ __global__ void __launch_bounds__(128) re_stage_kernel(const REStageArgs<T> a) {
         T xe4 = 0, fn4 = 0;
         T zbp6 = 0, zbp5 = 0, gg6 = 0, gg5 = 0;
 
+        // row r+1 is loaded while row r is computed (the loads of one iteration are in
+        // flight during the ~thousand instructions of the previous one)
+        T nh = 0, nhu = 0, nhv = 0, nzb = 0, nz = 0, nnb = 0, ng = 0;
+        bool nm = false;
+        auto load_row = [&](int rr) {
+            if (rr < L1 && colok) {
+                const long long i = (long long)rr * pitch + c;
+                nh = __ldg(a.h + i);
+                nhu = __ldg(a.hu + i);
+                nhv = __ldg(a.hv + i);
+                nzb = __ldg(a.zb + i);
+                nz = __ldg(a.z + i);
+                nnb = __ldg(a.nb + i);
+                if (!MPM) ng = __ldg(a.G + i);
+                if (HAS_MASK) nm = __ldg(a.nodata + i) != 0;
+            } else {
+                nh = nhu = nhv = nzb = nz = nnb = ng = T(0);
+                nm = false;
+            }
+        };
+        load_row(L0);
+
+#pragma unroll kRowUnroll
         for (int r = L0; r < L1 + 5; ++r) {
             const bool rowA = r < L1;
-            // ================= A: load row r, x-faces of row r, y-face (r-1 | r)
-            T h_r = 0, hu_r = 0, hv_r = 0, zb_r = 0, z_r = 0, nb_r = 0, g_r = 0;
-            bool m_r = false;
-            if (rowA && colok) {
-                const long long i = (long long)r * pitch + c;
-                h_r = a.h[i];
-                hu_r = a.hu[i];
-                hv_r = a.hv[i];
-                zb_r = a.zb[i];
-                z_r = a.z[i];
-                nb_r = a.nb[i];
-                if (!MPM) g_r = a.G[i];
-                if (HAS_MASK) m_r = a.nodata[i] != 0;
-            }
+            // ================= A: row r (prefetched), x-faces of row r, y-face (r-1 | r)
+            const T h_r = nh, hu_r = nhu, hv_r = nhv, zb_r = nzb, z_r = nz, nb_r = nnb, g_r = ng;
+            const bool m_r = nm;
+            load_row(r + 1);
             const HCell<T> pr = make_hcell(h_r, hu_r, hv_r, zb_r, z_r, nb_r);
             const T zt_r = z_r + zb_r;
             T xf0 = 0, xf1 = 0, xf2 = 0;
@@ -154,9 +176,15 @@ __global__ void __launch_bounds__(128) re_stage_kernel(const REStageArgs<T> a) {
                 T f0 = xfA0, f1 = xfA1, f2 = xfA2;
                 f0 = f0 + yM[0]; f1 = f1 + yM[1]; f2 = f2 + yM[2];      // south face upwM
                 f0 = f0 + nfA0; f1 = f1 + nfA1; f2 = f2 + nfA2;         // north face upwP
-                hr1 = hA - dt * f0 / dx;
-                hur1 = huA - dt * f1 / dx;
-                hvr1 = hvA - dt * f2 / dx;
+                if constexpr (is_f32<T>()) {
+                    hr1 = hA - dtdx * f0;
+                    hur1 = huA - dtdx * f1;
+                    hvr1 = hvA - dtdx * f2;
+                } else {
+                    hr1 = hA - dt * f0 / dx;
+                    hur1 = huA - dt * f1 / dx;
+                    hvr1 = hvA - dt * f2 / dx;
+                }
             }
 
             // ================= C: momentum corrections of row r-2
@@ -189,7 +217,7 @@ __global__ void __launch_bounds__(128) re_stage_kernel(const REStageArgs<T> a) {
             const int q = r - 3;
             const bool rowD = (q >= L0) && (q < L1);
             T hbh = hf3h, hbu = hf3u, hbv = hf3v, zb1 = zin3, gb1 = gin3;
-            if (a.ring != nullptr && rowD) {
+            if (rowD && (bc_strip || (a.ring != nullptr && (q == 0 || q == ny - 1)))) {
                 const int slot = colok ? ring_slot(q, c, ny, nx) : -1;
                 unsigned flags = 0;
                 int hdy = 0, hdx = 0, mdy = 0, mdx = 0, zdy = 0, zdx = 0, gdy = 0, gdx = 0;
@@ -243,7 +271,8 @@ __global__ void __launch_bounds__(128) re_stage_kernel(const REStageArgs<T> a) {
                 T acc = xe4;
                 acc = acc + (-fn4);  // north face (roe_exner.py:712)
                 acc = acc + Fy;      // south face (roe_exner.py:713)
-                zbp4 = e4.zb - dt * acc / dx;
+                if constexpr (is_f32<T>()) zbp4 = e4.zb - dtdx * acc;
+                else zbp4 = e4.zb - dt * acc / dx;
             }
             const T gg4 = e4.G;
 
@@ -251,7 +280,7 @@ __global__ void __launch_bounds__(128) re_stage_kernel(const REStageArgs<T> a) {
             const int p = r - 5;
             const bool rowG = (p >= L0) && (p < L1);
             T zfin = zbp5, gfin = gg5;
-            if (a.ring != nullptr && rowG) {
+            if (rowG && (bc_strip || (a.ring != nullptr && (p == 0 || p == ny - 1)))) {
                 const int slot = colok ? ring_slot(p, c, ny, nx) : -1;
                 unsigned flags = 0;
                 int zdy = 0, zdx = 0, gdy = 0, gdx = 0;
