@@ -174,6 +174,25 @@ int pxb_roe_run(pxb_roe_plan* plan, const pxb_roe_fields* a, const pxb_roe_field
                 int32_t scheme, double cfl, void* dt_log, void* stream);
 int pxb_roe_check(pxb_roe_plan* plan, void* stream);
 
+/* --- allocation-free time step ----------------------------------------------------- */
+/* No counterpart in the reference: PyExner's JAX step never manages device memory
+ * itself.  For callers that cannot allocate device memory when they need dt -- an XLA
+ * custom call, which must work inside the buffers XLA has already allocated; a host
+ * application whose policy forbids cudaMalloc after start-up; code recording a stream
+ * capture, which an allocation would break.  Same result as pxb_re_cfl, without a plan:
+ * dt = max(cfl * min over active faces of dx / speed, 1e-6), written to dt_dev (one
+ * element of dtype).  nodata may be NULL.  Calls no cudaMalloc/cudaFree: the reduction
+ * scratch is a fixed array of (8192 + 32) * 8 bytes in device memory owned by the
+ * library, resident on every device that loads it until the process exits.  Grids up
+ * to 31 * 8192 = 253952 columns wide (any height); wider grids return PXB_ERR_ARG.
+ * The first call on a device looks up the array's device address; make that first call
+ * before any stream capture.  All calls share the array: calls whose kernels can
+ * overlap on the GPU (unordered streams, or several host threads on one device) race
+ * and must be serialised by the caller. */
+int pxb_re_cfl_noalloc(int32_t ny, int32_t nx, int64_t pitch, int32_t dtype, double dx, double cfl,
+                       const void* h, const void* hu, const void* hv, const void* G, const uint8_t* nodata,
+                       void* dt_dev, void* stream);
+
 /* --- misc ------------------------------------------------------------------------- */
 const char* pxb_last_error(void);
 int pxb_version(void);

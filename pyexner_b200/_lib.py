@@ -100,6 +100,8 @@ SIGNATURES = {
     "pxb_roe_stage": [c_void_p, POINTER(RoeFields), POINTER(RoeFields), POINTER(RoeFields), c_void_p, c_void_p],
     "pxb_roe_run": [c_void_p, POINTER(RoeFields), POINTER(RoeFields), c_int32, c_int32, c_double, c_void_p, c_void_p],
     "pxb_roe_check": [c_void_p, c_void_p],
+    "pxb_re_cfl_noalloc": [c_int32, c_int32, c_int64, c_int32, c_double, c_double, c_void_p, c_void_p, c_void_p,
+                           c_void_p, c_void_p, c_void_p, c_void_p],
     "pxb_version": [],
 }
 

@@ -25,6 +25,7 @@ UNITS = [
     ("kernels_f32.cu", []),
     ("kernels_f64.cu", ["-fmad=false"]),
     ("capi.cu", []),
+    ("noalloc.cu", []),
 ]
 
 

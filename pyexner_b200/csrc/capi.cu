@@ -443,6 +443,10 @@ int run_graph(PlanCommon& P, const std::vector<const void*>& key, int reps, cuda
 
 }  // namespace
 
+namespace pxb {
+int set_error(int code, const std::string& msg) { return fail(code, msg); }
+}  // namespace pxb
+
 // =====================================================================================
 struct pxb_re_plan {
     PlanCommon c;

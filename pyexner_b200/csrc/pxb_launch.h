@@ -7,7 +7,12 @@
 #include "re_stage.cuh"
 #include "roe_plain.cuh"
 
+#include <string>
+
 namespace pxb {
+
+// Records the message returned by pxb_last_error() on this thread; returns `code`.
+int set_error(int code, const std::string& msg);
 
 template <class T>
 cudaError_t launch_re_stage(const REStageArgs<T>& a, bool mpm, bool has_mask, bool avg, int grid, cudaStream_t s);

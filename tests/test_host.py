@@ -71,3 +71,13 @@ def test_gaussian_bed_case_is_seeded():
     assert a["h"].shape == (64, 64)
     assert np.all(a["z_b"] >= 0.05 - 1e-12)
     assert np.allclose(a["hu"], 0.1 * a["h"])
+
+
+def test_noalloc_rejects_too_wide_grid_without_touching_the_gpu():
+    """The allocation-free time step checks the grid against its fixed scratch first."""
+    if not os.path.exists(_lib.LIB_PATH):
+        pytest.skip("library not built")
+    lib = _lib.load()
+    code = lib.pxb_re_cfl_noalloc(10, 300000, 300000, _lib.F32, 0.1, 0.5, None, None, None, None, None, None, None)
+    assert code == _lib.ERR_ARG
+    assert b"allocation-free limit" in lib.pxb_last_error()
