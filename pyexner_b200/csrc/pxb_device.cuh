@@ -125,18 +125,24 @@ __device__ __forceinline__ void roe_exner_face(const HCell<T>& I, const HCell<T>
     T l1 = l1r, lE1 = T(0);
     const T ei = uhi - I.c, ej = uhj - J.c;
     const bool m1 = (ei < T(0)) && (ej > T(0));
-    if (m1) {
-        const T t = ei * (ej - l1r) / (ej - ei);
-        lE1 = l1r - t;
-        l1 = t;
-    }
     T l3 = l3r, lE3 = T(0);
     const T fi = uhi + I.c, fj = uhj + J.c;
     const bool m3 = (fi < T(0)) && (fj > T(0));
-    if (m3) {
-        const T num = fj * (l3r - fi);
-        lE3 = l3r - num / (fj - fi);
-        l3 = num / ((fj - fi) + T(VEL_TOL));
+    // transonic faces are rare: the float build skips the block for the whole warp
+    // when no lane needs it (all lanes evaluate every face, so the vote is safe)
+    bool need = true;
+    if constexpr (is_f32<T>()) need = __any_sync(FULL, m1 || m3);
+    if (need) {
+        if (m1) {
+            const T t = ei * (ej - l1r) / (ej - ei);
+            lE1 = l1r - t;
+            l1 = t;
+        }
+        if (m3) {
+            const T num = fj * (l3r - fi);
+            lE3 = l3r - num / (fj - fi);
+            l3 = num / ((fj - fi) + T(VEL_TOL));
+        }
     }
     const T dh = J.h - I.h;
     const T dhu = J.h * uhj - I.h * uhi;
@@ -274,13 +280,10 @@ __device__ __forceinline__ T exner_face(const ECell<T>& I, const ECell<T>& J) {
     const bool big = fabs(dz) > T(SED_TOL);
     bool up;
     if constexpr (is_f32<T>()) {
-        if (big) {
-            const float dq = mul_rn(mul_rn(gt, J.um), uhj) - mul_rn(mul_rn(gt, I.um), uhi);
-            up = (dq == 0.f) || (dq == dq && ((dq > 0.f) == (dz > 0.f)));
-        } else {
-            const float num = mul_rn(uhi, I.sq) + mul_rn(uhj, J.sq);  // sign of ut (denominator > 0)
-            up = num >= 0.f;
-        }
+        const float dq = mul_rn(mul_rn(gt, J.um), uhj) - mul_rn(mul_rn(gt, I.um), uhi);
+        const bool up_big = (dq == 0.f) || (dq == dq && ((dq > 0.f) == (dz > 0.f)));
+        const float num = mul_rn(uhi, I.sq) + mul_rn(uhj, J.sq);  // sign of ut (denominator > 0)
+        up = big ? up_big : (num >= 0.f);
     } else {
         const T ut = (uhi * I.sq + uhj * J.sq) / (I.sq + J.sq);
         const T dq = gt * J.um * uhj - gt * I.um * uhi;
@@ -336,12 +339,17 @@ __device__ __forceinline__ T mpm_grass(T h, T hu, T hv, bool nodata, const SedTa
         float rcb = f_ex2(-0.33333333333f * f_lg2(hc));  // h^(-1/3)
         rcb = rcb * (4.f - hc * rcb * rcb * rcb) * (1.f / 3.f);
         float G = 0.f;
-        for (int k = 0; k < S.n; ++k) {
-            const float th = fmaxf(S.k_theta[k] * vel2 * rcb, 0.f);
-            const float dth = th - S.s[k].thc;
-            if (dth > 0.f) {
-                const float th15 = th * f_sqrt(th);
-                G += S.k_g1[k] * rs * f_sqrt(dth) * dth * f_rcp(th15 + 1e-5f);
+#pragma unroll
+        for (int k = 0; k < PXB_MAX_SED; ++k) {
+            if (k < S.n) {
+                const float th = fmaxf(S.k_theta[k] * vel2 * rcb, 0.f);
+                const float dth = th - S.s[k].thc;
+                // below the Shields threshold G is 0: skip the block when no lane is above it
+                if (__any_sync(FULL, dth > 0.f)) {
+                    const float pos = dth > 0.f ? dth : 0.f;
+                    const float th15 = th * f_sqrt(th);
+                    G += S.k_g1[k] * rs * f_sqrt(pos) * pos * f_rcp(th15 + 1e-5f);
+                }
             }
         }
         G *= S.inv_one_minus_por;

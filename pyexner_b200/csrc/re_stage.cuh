@@ -19,15 +19,16 @@
 // the layouts the host accepts).  Every face is evaluated once per warp; the only
 // redundant work is the 6 halo columns of each strip and 6 halo rows of each band.
 #pragma once
+#include <type_traits>
+
 #include "pxb_device.cuh"
 
-#ifndef PXB_ROW_UNROLL
-#define PXB_ROW_UNROLL 1
+// Resident 128-thread blocks per SM the float build is register-limited to (tuning knob).
+#ifndef PXB_STAGE_MIN_BLOCKS
+#define PXB_STAGE_MIN_BLOCKS 5
 #endif
 
 namespace pxb {
-
-constexpr int kRowUnroll = PXB_ROW_UNROLL;
 
 template <class T>
 struct REStageArgs {
@@ -78,7 +79,7 @@ __device__ __forceinline__ ECell<T> shfl_down_ecell(const ECell<T>& p) {
 }
 
 template <class T, bool MPM, bool HAS_MASK, bool AVG>
-__global__ void __launch_bounds__(128) re_stage_kernel(const REStageArgs<T> a) {
+__global__ void __launch_bounds__(128, PXB_STAGE_MIN_BLOCKS) re_stage_kernel(const REStageArgs<T> a) {
     const int lane = threadIdx.x & 31;
     const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -141,9 +142,11 @@ __global__ void __launch_bounds__(128) re_stage_kernel(const REStageArgs<T> a) {
         };
         load_row(L0);
 
-#pragma unroll kRowUnroll
-        for (int r = L0; r < L1 + 5; ++r) {
-            const bool rowA = r < L1;
+        // One pipeline iteration.  In the steady state (rows L0+5 .. L1-1) every phase has
+        // valid rows, so the row checks compile away.
+        auto iterate = [&](const int r, auto steady_tag) {
+            constexpr bool S = decltype(steady_tag)::value;
+            const bool rowA = S || r < L1;
             // ================= A: row r (prefetched), x-faces of row r, y-face (r-1 | r)
             const T h_r = nh, hu_r = nhu, hv_r = nhv, zb_r = nzb, z_r = nz, nb_r = nnb, g_r = ng;
             const bool m_r = nm;
@@ -156,8 +159,10 @@ __global__ void __launch_bounds__(128) re_stage_kernel(const REStageArgs<T> a) {
                 const T he = __shfl_down_sync(FULL, h_r, 1);
                 const bool me = HAS_MASK ? (__shfl_down_sync(FULL, (int)m_r, 1) != 0) : false;
                 const bool xact = rowA && has_e && ((h_r > DRY) || (he > DRY)) && !(m_r || me);
-                T P[3] = {T(0), T(0), T(0)}, M[3] = {T(0), T(0), T(0)};
-                if (xact) roe_exner_face<T, false>(pr, pe, dx, P, M);
+                T P[3], M[3];
+                roe_exner_face<T, false>(pr, pe, dx, P, M);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) { P[k] = xact ? P[k] : T(0); M[k] = xact ? M[k] : T(0); }
                 const T w0 = __shfl_up_sync(FULL, P[0], 1);
                 const T w1 = __shfl_up_sync(FULL, P[1], 1);
                 const T w2 = __shfl_up_sync(FULL, P[2], 1);
@@ -166,13 +171,15 @@ __global__ void __launch_bounds__(128) re_stage_kernel(const REStageArgs<T> a) {
                 if (xact) { xf0 = xf0 + M[0]; xf1 = xf1 + M[1]; xf2 = xf2 + M[2]; }
                 if (wact) { xf0 = xf0 + w0; xf1 = xf1 + w1; xf2 = xf2 + w2; }
             }
-            T yP[3] = {T(0), T(0), T(0)}, yM[3] = {T(0), T(0), T(0)};
-            const bool yact = rowA && (r - 1 >= L0) && colok && ((hA > DRY) || (h_r > DRY)) && !((mwin & 1u) || m_r);
-            if (yact) roe_exner_face<T, true>(pA, pr, dx, yP, yM);
+            T yP[3], yM[3];
+            const bool yact = rowA && (S || r - 1 >= L0) && colok && ((hA > DRY) || (h_r > DRY)) && !((mwin & 1u) || m_r);
+            roe_exner_face<T, true>(pA, pr, dx, yP, yM);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) { yP[k] = yact ? yP[k] : T(0); yM[k] = yact ? yM[k] : T(0); }
 
             // ================= B: hydro update of row r-1
             T hr1 = 0, hur1 = 0, hvr1 = 0;
-            if (r - 1 >= L0 && r - 1 < L1) {
+            if (S || (r - 1 >= L0 && r - 1 < L1)) {
                 T f0 = xfA0, f1 = xfA1, f2 = xfA2;
                 f0 = f0 + yM[0]; f1 = f1 + yM[1]; f2 = f2 + yM[2];      // south face upwM
                 f0 = f0 + nfA0; f1 = f1 + nfA1; f2 = f2 + nfA2;         // north face upwP
@@ -196,7 +203,7 @@ __global__ void __launch_bounds__(128) re_stage_kernel(const REStageArgs<T> a) {
                 const bool m2 = HAS_MASK && ((mwin >> 1) & 1u);
                 const bool mE = HAS_MASK ? (__shfl_down_sync(FULL, (int)m2, 1) != 0) : false;
                 const bool mW = HAS_MASK ? (__shfl_up_sync(FULL, (int)m2, 1) != 0) : false;
-                if (q2 >= L0 && q2 < L1) {
+                if (S || (q2 >= L0 && q2 < L1)) {
                     hf2h = hr2;
                     hf2u = hur2;
                     hf2v = hvr2;
@@ -215,7 +222,7 @@ __global__ void __launch_bounds__(128) re_stage_kernel(const REStageArgs<T> a) {
 
             // ================= D: first boundary application on row q = r-3
             const int q = r - 3;
-            const bool rowD = (q >= L0) && (q < L1);
+            const bool rowD = S || ((q >= L0) && (q < L1));
             T hbh = hf3h, hbu = hf3u, hbv = hf3v, zb1 = zin3, gb1 = gin3;
             if (rowD && (bc_strip || (a.ring != nullptr && (q == 0 || q == ny - 1)))) {
                 const int slot = colok ? ring_slot(q, c, ny, nx) : -1;
@@ -255,19 +262,21 @@ __global__ void __launch_bounds__(128) re_stage_kernel(const REStageArgs<T> a) {
                 const ECell<T> ee = shfl_down_ecell(e3);
                 const bool mqe = HAS_MASK ? (__shfl_down_sync(FULL, (int)mq, 1) != 0) : false;
                 const bool xact = rowD && has_e && exner_active(e3, ee, mq, mqe);
-                const T F = xact ? exner_face<T, false>(e3, ee) : T(0);
+                const T Fx = exner_face<T, false>(e3, ee);
+                const T F = xact ? Fx : T(0);
                 const T Fw = __shfl_up_sync(FULL, F, 1);
                 const bool wact = (__shfl_up_sync(FULL, (int)xact, 1) != 0) && lane > 0;
                 // roe_exner.py:710-711: -F of the west face first, then +F of the east face
                 if (wact) xe3 = xe3 + (-Fw);
                 if (xact) xe3 = xe3 + F;
             }
-            const bool yex = rowD && (q - 1 >= L0) && colok && exner_active(e4, e3, mq1, mq);
-            const T Fy = yex ? exner_face<T, true>(e4, e3) : T(0);
+            const bool yex = rowD && (S || q - 1 >= L0) && colok && exner_active(e4, e3, mq1, mq);
+            const T Fyv = exner_face<T, true>(e4, e3);
+            const T Fy = yex ? Fyv : T(0);
 
             // ================= F: z_b update of row r-4
             T zbp4 = 0;
-            if (r - 4 >= L0 && r - 4 < L1) {
+            if (S || (r - 4 >= L0 && r - 4 < L1)) {
                 T acc = xe4;
                 acc = acc + (-fn4);  // north face (roe_exner.py:712)
                 acc = acc + Fy;      // south face (roe_exner.py:713)
@@ -278,7 +287,7 @@ __global__ void __launch_bounds__(128) re_stage_kernel(const REStageArgs<T> a) {
 
             // ================= G: second boundary application and stores of row p = r-5
             const int p = r - 5;
-            const bool rowG = (p >= L0) && (p < L1);
+            const bool rowG = S || ((p >= L0) && (p < L1));
             T zfin = zbp5, gfin = gg5;
             if (rowG && (bc_strip || (a.ring != nullptr && (p == 0 || p == ny - 1)))) {
                 const int slot = colok ? ring_slot(p, c, ny, nx) : -1;
@@ -334,7 +343,12 @@ __global__ void __launch_bounds__(128) re_stage_kernel(const REStageArgs<T> a) {
             e4 = e3; xe4 = xe3; fn4 = Fy;
             zbp6 = zbp5; zbp5 = zbp4;
             gg6 = gg5; gg5 = gg4;
-        }
+        };
+        const int steady0 = min(L0 + 5, L1), steady1 = L1;
+        int r = L0;
+        for (; r < steady0; ++r) iterate(r, std::false_type{});
+        for (; r < steady1; ++r) iterate(r, std::true_type{});
+        for (; r < L1 + 5; ++r) iterate(r, std::false_type{});
     }
     if (bad) atomicOr(a.err, 1);
 }
