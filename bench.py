@@ -16,11 +16,12 @@ Reported:
              duration, against the measured HBM copy bandwidth;
   fp64       the same loop in float64 (the plain FP64 GPU path) and its speed ratio;
   accuracy   rel-L1 of h and z+z_b, float32 vs float64 after the accuracy run;
-  cpu_baseline  the float64 NumPy oracle on a bounded sample on the host cores.
+  cpu_baseline  the float64 C/OpenMP oracle (all host threads) on a 512 x 512 sample of
+             the same generator, about 10 s of CPU work.
 
 ``--impl reference`` times the reference algorithm on the CPU instead (the float64
-oracle restatement of PyExner's JAX step; JAX itself is not installed on these hosts)
-and prints its line with "impl": "reference".
+C/OpenMP restatement of PyExner's JAX step, oracle/c; JAX itself is not installed on
+these hosts) and prints its line with "impl": "reference".
 """
 from __future__ import annotations
 
@@ -56,57 +57,92 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle samples while the timed region runs."""
+    """SM clock and clock-event (throttle) reasons sampled while the timed region runs.
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    Reads NVML in a host thread every 2 ms (read-only queries); falls back to
+    ``nvidia-smi -lms 100`` when NVML is unavailable."""
 
     def __init__(self, index=0):
         self.index = index
+        self.sm = []
+        self.max = None
+        self.reasons = set()
+        self._stop = threading.Event()
+        self._nvml = None
         self.proc = None
         self.lines = []
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+            import pynvml
+
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            names = {pynvml.nvmlClocksEventReasonHwSlowdown: "hw_slowdown",
+                     pynvml.nvmlClocksEventReasonHwThermalSlowdown: "hw_thermal_slowdown",
+                     pynvml.nvmlClocksEventReasonSwThermalSlowdown: "sw_thermal_slowdown",
+                     pynvml.nvmlClocksEventReasonSwPowerCap: "sw_power_cap"}
+
+            def run():
+                while not self._stop.is_set():
+                    try:
+                        self.sm.append(float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)))
+                        r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        for bit, nm in names.items():
+                            if r & bit:
+                                self.reasons.add(nm)
+                    except Exception:
+                        pass
+                    time.sleep(0.002)
+
+            self._nvml = pynvml
+            self.t = threading.Thread(target=run, daemon=True)
+            self.t.start()
+        except Exception:
+            self._start_smi()
+        return self
+
+    def _start_smi(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t = threading.Thread(target=lambda: [self.lines.append(l.strip()) for l in self.proc.stdout],
+                                      daemon=True)
             self.t.start()
         except FileNotFoundError:
             self.proc = None
-        return self
-
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
 
     def __exit__(self, *a):
+        self._stop.set()
         if self.proc is not None:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        elif self._nvml is not None:
+            self.t.join(timeout=1)
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for l in self.lines:
             parts = [p.strip() for p in l.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 6:
                 continue
             try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
+                self.sm.append(float(parts[0]))
+                self.max = float(parts[1])
             except ValueError:
                 continue
-            for nm, v in zip(names, parts[5:9]):
+            for nm, v in zip(names, parts[2:6]):
                 if v.lower().startswith("active"):
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                    self.reasons.add(nm)
+        return {"sm_mhz": statistics.median(self.sm) if self.sm else None, "sm_max_mhz": self.max,
+                "reasons": sorted(self.reasons), "samples": len(self.sm)}
 
 
 def build_case(n, dtype, device):
@@ -248,11 +284,9 @@ def accuracy_run(n, steps):
             "hu_rel_l1": l1(a["hu"][s], b["hu"][s])}
 
 
-def cpu_oracle_sample(n=256, steps=2):
-    """Float64 NumPy oracle (single thread) on the same generator at n x n."""
+def _oracle_case(n):
     from oracle import boundaries as OB
-    from oracle import integrators as OI
-    from oracle import roe_exner as ORE
+    from oracle import c_oracle as CO
     from pyexner_b200 import cases
 
     c = cases.gaussian_bed(n)
@@ -261,32 +295,52 @@ def cpu_oracle_sample(n=256, steps=2):
     st["n_b"] = np.zeros_like(st["h"])
     st["seds"] = c["seds"]
     mask = OB.roe_exner_mask(st["z"].copy(), bcs.boundary_mask)
-    st = ORE.init(st, mask, bcs, True)
-    OI.run_roe_exner(st, mask, bcs, True, c["dx"], 0.5, 1, "SSPRK2")  # warm-up
-    t0 = time.perf_counter()
-    OI.run_roe_exner(st, mask, bcs, True, c["dx"], 0.5, steps, "SSPRK2")
-    sec = time.perf_counter() - t0
-    return n * n * steps / sec, f"{n}x{n} Gaussian-bed case, {steps} SSPRK2 steps, float64 NumPy oracle"
+    st = CO.init(st, mask, bcs, True, c["dx"])
+    return c, bcs, st, mask
+
+
+def cpu_oracle_sample(n=512, budget_s=10.0, min_steps=3):
+    """Float64 C/OpenMP oracle (all host threads) on the same generator at n x n,
+    SSPRK2 steps until ``budget_s`` seconds of CPU work."""
+    from oracle import c_oracle as CO
+
+    c, bcs, st, mask = _oracle_case(n)
+    CO.run_roe_exner(st, mask, bcs, True, c["dx"], 0.5, 1, "SSPRK2")  # warm-up
+    steps, sec = 0, 0.0
+    while sec < budget_s or steps < min_steps:
+        t0 = time.perf_counter()
+        st, _ = CO.run_roe_exner(st, mask, bcs, True, c["dx"], 0.5, 1, "SSPRK2")
+        sec += time.perf_counter() - t0
+        steps += 1
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return n * n * steps / sec, cores, (f"{n}x{n} Gaussian-bed case (same generator), {steps} SSPRK2 steps, "
+                                        f"float64 C/OpenMP restatement of the reference step, {cores} threads")
 
 
 def reference_arm(args):
+    """The reference's algorithm on the host cores: the float64 C/OpenMP restatement of
+    PyExner's step (JAX, which runs the reference itself, is not installed here), on a
+    512 x 512 sample of the same workload; one timed step = one SSPRK2 step."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    n = 256
-    per = []
-    for _ in range(args.warmup):
-        cpu_oracle_sample(n, 1)
-    for _ in range(args.steps):
-        v, sample = cpu_oracle_sample(n, 1)
-        per.append(v)
-    v = float(np.mean(per))
+    from oracle import c_oracle as CO
+
+    n = 512
+    c, bcs, st, mask = _oracle_case(n)
+    st, _ = CO.run_roe_exner(st, mask, bcs, True, c["dx"], 0.5, max(1, args.warmup), "SSPRK2")
+    t0 = time.perf_counter()
+    st, _ = CO.run_roe_exner(st, mask, bcs, True, c["dx"], 0.5, args.steps, "SSPRK2")
+    sec = time.perf_counter() - t0
+    v = n * n * args.steps / sec
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    sample = f"{n}x{n} sample of the Gaussian-bed case, {args.steps} SSPRK2 steps, float64, {cores} threads"
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * n * n / v,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded Gaussian bed)",
-            "config": {"workload": f"roe_exner_gaussian_bed_{n}x{n}_ssprk2 (bounded CPU sample of the 2048x2048 case)"},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
+            "config": {"workload": "roe_exner_gaussian_bed_2048x2048_mpm_ssprk2 (512x512 CPU sample)"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -388,8 +442,8 @@ def main():
         return
     cpu = None
     if not args.no_cpu:
-        v, sample = cpu_oracle_sample(256, 2)
-        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample}
+        v, cores, sample = cpu_oracle_sample(512, 10.0)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps, "higher_is_better": True,

@@ -370,6 +370,7 @@ int common_setup(PlanCommon& P, int ny, int nx, long long pitch, int dtype, doub
                  int nh, bool roe) {
     if (ny < 3 || nx < 3) return fail(PXB_ERR_ARG, "grid must be at least 3 x 3 cells including the ring");
     if (pitch < nx) return fail(PXB_ERR_ARG, "pitch smaller than nx");
+    if ((long long)ny * pitch >= (1LL << 31)) return fail(PXB_ERR_ARG, "planes of 2^31 elements or more are not supported");
     if (dtype != PXB_F32 && dtype != PXB_F64) return fail(PXB_ERR_ARG, "dtype must be PXB_F32 or PXB_F64");
     if (!(dx > 0) || !std::isfinite(dx)) return fail(PXB_ERR_ARG, "dx must be positive and finite");
     if (nh < 0 || (nh > 0 && !hs)) return fail(PXB_ERR_ARG, "handlers pointer is null");

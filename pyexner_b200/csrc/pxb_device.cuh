@@ -174,22 +174,22 @@ __device__ __forceinline__ void roe_exner_face(const HCell<T>& I, const HCell<T>
     // Upwinded waves (roe_exner.py:484-507); P columns (1,l1,vt), (0,0,ct), (1,l3,vt).
     T p0 = T(0), p1 = T(0), p2 = T(0), n0 = T(0), n1 = T(0), n2 = T(0);
     if constexpr (is_f32<T>()) {
-        // branch-free: each wave goes to one side by its speed's sign (NaN speeds to none)
-        const float w1 = l1 * a1 - b1, w2 = ut * a2, w3 = l3 * a3 - b3;
-        const float e1 = m1 ? lE1 * a1 : 0.f, e3 = m3 ? lE3 * a3 : 0.f;
-        const bool s1 = l1 > 0.f, s2 = ut > 0.f, s3 = l3 > 0.f, t1 = lE1 > 0.f, t3 = lE3 > 0.f;
-        const bool z1 = l1 <= 0.f, z2 = ut <= 0.f, z3 = l3 <= 0.f;
-        const float q0a = s1 ? w1 : 0.f, q0b = s3 ? w3 : 0.f;
-        const float r0a = z1 ? w1 : 0.f, r0b = z3 ? w3 : 0.f;
-        const float ep1 = t1 ? e1 : 0.f, en1 = t1 ? 0.f : e1;
-        const float ep3 = t3 ? e3 : 0.f, en3 = t3 ? 0.f : e3;
-        p0 = q0a + q0b + ep1 + ep3;
-        n0 = r0a + r0b + en1 + en3;
-        p1 = q0a * l1 + q0b * l3 + ep1 * l1 + ep3 * l3;
-        n1 = r0a * l1 + r0b * l3 + en1 * l1 + en3 * l3;
-        const float wc = w2 * ct;
-        p2 = (q0a + q0b + ep1 + ep3) * vt + (s2 ? wc : 0.f);
-        n2 = (r0a + r0b + en1 + en3) * vt + (z2 ? wc : 0.f);
+        // Branch-free split.  With A_k = [lambda_k > 0] w_k + [lambda_E,k > 0] e_k and
+        // T_k = w_k + e_k (k = 1, 3; e_k = lambda_E,k alpha_k, zero without the fix):
+        //   upwP = (A1 + A3, A1 l1 + A3 l3, (A1 + A3) vt + [ut > 0] w2 ct)
+        //   upwM = the same with T_k - A_k and [ut <= 0].
+        const float w1 = l1 * a1 - b1, w2c = ut * a2 * ct, w3 = l3 * a3 - b3;
+        const float e1 = lE1 * a1, e3 = lE3 * a3;
+        const float A1 = (l1 > 0.f ? w1 : 0.f) + (lE1 > 0.f ? e1 : 0.f);
+        const float A3 = (l3 > 0.f ? w3 : 0.f) + (lE3 > 0.f ? e3 : 0.f);
+        const float B1 = (w1 + e1) - A1, B3 = (w3 + e3) - A3;
+        const bool s2 = ut > 0.f;
+        p0 = A1 + A3;
+        p1 = A1 * l1 + A3 * l3;
+        p2 = p0 * vt + (s2 ? w2c : 0.f);
+        n0 = B1 + B3;
+        n1 = B1 * l1 + B3 * l3;
+        n2 = n0 * vt + (s2 ? 0.f : w2c);
     } else {
     {
         const T w = l1 * a1 - b1;

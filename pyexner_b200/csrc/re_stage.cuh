@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(128, PXB_STAGE_MIN_BLOCKS) re_stage_kernel(con
     const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     const int ny = a.ny, nx = a.nx;
-    const long long pitch = a.pitch;
+    const unsigned upitch = (unsigned)a.pitch;  // planes are < 2^31 elements (checked at plan creation)
     const T dt = *a.dt;
     const T dx = a.dx;
     const T dtdx = dt / dx;  // float path only
@@ -106,6 +106,7 @@ __global__ void __launch_bounds__(128, PXB_STAGE_MIN_BLOCKS) re_stage_kernel(con
         const int L0 = max(0, R0 - 3), L1 = min(ny, R1 + 3);
         // boundary recipes can only apply in the first/last strip or on rows 0 / ny-1
         const bool bc_strip = (a.ring != nullptr) && (strip == 0 || last_strip);
+        const bool bc_rows = (a.ring != nullptr) && (R0 == 0 || R1 == ny);
 
         // ---- carried pipeline state
         HCell<T> pA = make_hcell(T(0), T(0), T(0), T(0), T(0), T(0));
@@ -126,7 +127,7 @@ __global__ void __launch_bounds__(128, PXB_STAGE_MIN_BLOCKS) re_stage_kernel(con
         bool nm = false;
         auto load_row = [&](int rr) {
             if (rr < L1 && colok) {
-                const long long i = (long long)rr * pitch + c;
+                const unsigned i = (unsigned)rr * upitch + (unsigned)c;
                 nh = __ldg(a.h + i);
                 nhu = __ldg(a.hu + i);
                 nhv = __ldg(a.hv + i);
@@ -224,7 +225,7 @@ __global__ void __launch_bounds__(128, PXB_STAGE_MIN_BLOCKS) re_stage_kernel(con
             const int q = r - 3;
             const bool rowD = S || ((q >= L0) && (q < L1));
             T hbh = hf3h, hbu = hf3u, hbv = hf3v, zb1 = zin3, gb1 = gin3;
-            if (rowD && (bc_strip || (a.ring != nullptr && (q == 0 || q == ny - 1)))) {
+            if (rowD && (bc_strip || (bc_rows && (q == 0 || q == ny - 1)))) {
                 const int slot = colok ? ring_slot(q, c, ny, nx) : -1;
                 unsigned flags = 0;
                 int hdy = 0, hdx = 0, mdy = 0, mdx = 0, zdy = 0, zdx = 0, gdy = 0, gdx = 0;
@@ -289,7 +290,7 @@ __global__ void __launch_bounds__(128, PXB_STAGE_MIN_BLOCKS) re_stage_kernel(con
             const int p = r - 5;
             const bool rowG = S || ((p >= L0) && (p < L1));
             T zfin = zbp5, gfin = gg5;
-            if (rowG && (bc_strip || (a.ring != nullptr && (p == 0 || p == ny - 1)))) {
+            if (rowG && (bc_strip || (bc_rows && (p == 0 || p == ny - 1)))) {
                 const int slot = colok ? ring_slot(p, c, ny, nx) : -1;
                 unsigned flags = 0;
                 int zdy = 0, zdx = 0, gdy = 0, gdx = 0;
@@ -306,7 +307,7 @@ __global__ void __launch_bounds__(128, PXB_STAGE_MIN_BLOCKS) re_stage_kernel(con
                 }
             }
             if (rowG && p >= R0 && p < R1 && out_col) {
-                const long long i = (long long)p * pitch + c;
+                const unsigned i = (unsigned)p * upitch + (unsigned)c;
                 if (AVG) {
                     zfin = T(0.5) * a.azb[i] + T(0.5) * zfin;
                     if (a.oG) gfin = T(0.5) * a.aG[i] + T(0.5) * gfin;
@@ -316,7 +317,7 @@ __global__ void __launch_bounds__(128, PXB_STAGE_MIN_BLOCKS) re_stage_kernel(con
                 bad |= !d_isfinite(zfin);
             }
             if (rowD && q >= R0 && q < R1 && out_col) {
-                const long long i = (long long)q * pitch + c;
+                const unsigned i = (unsigned)q * upitch + (unsigned)c;
                 T oh = hbh, ou = hbu, ov = hbv;
                 if (AVG) {
                     oh = T(0.5) * a.ah[i] + T(0.5) * oh;

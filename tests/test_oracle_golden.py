@@ -107,3 +107,20 @@ def test_roe_step(request, case):
     same(dts, d["rk_dts"])
     for k in R.FIELDS:
         same(out[k], d[f"rk_{k}"])
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_c_oracle_matches_golden(request, case):
+    """The C/OpenMP restatement (CPU baseline) against the same golden vectors."""
+    from oracle import c_oracle as CO
+
+    d, bcs, mask, st, mpm = load_re_case(request.config.rootpath, case)
+    st = CO.init(st, mask, bcs, mpm, 0.1)
+    for k in RE.STATE_FIELDS:
+        assert np.max(np.abs(st[k] - d[f"init_{k}"])) <= 1e-14 * max(1.0, np.max(np.abs(d[f"init_{k}"])))
+    for scheme, tag in (("FE", "fe"), ("SSPRK2", "rk")):
+        out, dts = CO.run_roe_exner(st, mask, bcs, mpm, 0.1, 0.5, NSTEPS, scheme)
+        assert np.max(np.abs(dts - d[f"{tag}_dts"])) <= 1e-15
+        for k in RE.STATE_FIELDS:
+            ref = d[f"{tag}_{k}"]
+            assert np.max(np.abs(out[k] - ref)) <= 1e-13 * max(1e-300, np.max(np.abs(ref))), k
