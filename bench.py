@@ -367,6 +367,8 @@ def main():
     ap.add_argument("--n", type=int, default=2048)
     ap.add_argument("--impl", default="b200")
     ap.add_argument("--accuracy-steps", type=int, default=2000)
+    ap.add_argument("--n-big", type=int, default=8192, help="side of the bandwidth case (0 to skip)")
+    ap.add_argument("--big-steps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="short fixed sequence for ncu: build the case, run --warmup SSPRK2 steps, exit")
@@ -426,6 +428,20 @@ def main():
                 tk[k.strip()] = float(val)
         if "traffic_bytes_stage1_2048" in tk and "traffic_bytes_stage2_2048" in tk:
             traffic = 0.5 * (tk["traffic_bytes_stage1_2048"] + tk["traffic_bytes_stage2_2048"])
+    # ---- the 8192 x 8192 bandwidth case (same generator, 500-step configuration; K steps timed)
+    big = None
+    if args.n_big > 0:
+        cb, bb, cfgb, maskb, stb = build_case(args.n_big, torch.float32, "cuda")
+        secb, bscr = timed_device_loop(stb, maskb, cfgb, args.big_steps, args.warmup, flush)
+        ktb = kernel_breakdown(stb, bscr, maskb, cfgb, max(3, args.big_steps // 2), flush)
+        nb = args.n_big * args.n_big
+        achb = 0.5 * (WORDS_STAGE1 + WORDS_STAGE2) * esz * nb / (0.5 * (ktb["stage1"] + ktb["stage2"])) / 1e9
+        big = {"workload": f"roe_exner_gaussian_bed_{args.n_big}x{args.n_big}_mpm_ssprk2_f32",
+               "value": nb * args.big_steps / secb, "unit": UNIT, "steps": args.big_steps,
+               "roofline": {"achieved": achb, "peak": hbm, "unit": "GB/s", "frac": achb / hbm},
+               "ms": {k: 1e3 * v for k, v in ktb.items()}}
+        del stb, bscr
+        torch.cuda.empty_cache()
     # ---- float64 device loop, same config
     c64, b64, cfg64, mask64, st64 = build_case(n, torch.float64, "cuda")
     sec64, _ = timed_device_loop(st64, mask64, cfg64, max(3, args.steps // 2), args.warmup, flush)
@@ -456,6 +472,7 @@ def main():
                      "algorithmic_bytes_per_launch": stage_bytes,
                      "ms": {k: 1e3 * v for k, v in kt.items()}},
         "fp64": {"value": value64, "unit": UNIT, "fp32_over_fp64": value / world / value64},
+        "bandwidth_case": big,
         "accuracy": acc,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,

@@ -204,20 +204,19 @@ Resolved resolve(const pxb_bc_handler* hs, int nh, int ny, int nx, long long pit
         for (auto& kv : mp) {
             const long long cell = kv.first;
             const CellExpr& e = kv.second;
+            // The kernel evaluates the second pass in registers from first-pass values of
+            // donors in the same row (the cell itself included); a donor in another row
+            // must not be a hydro boundary cell, so that its value is the same in both passes.
             auto bad = [&](const GroupExpr& g, GroupExpr CellExpr::*grp) {
-                if (!g.set || g.is_const) return false;
-                if (g.src == cell) {
-                    if (grp == &CellExpr::mom) return !(g.m[0] == 1 && g.m[1] == 0 && g.m[2] == 0 && g.m[3] == 1);
-                    return false;
-                }
+                if (!g.set || g.is_const || g.src / nx == cell / nx) return false;
                 auto it = mp.find(g.src);
                 return it != mp.end() && ((it->second).*grp).set;
             };
             if (bad(e.h, &CellExpr::h) || bad(e.mom, &CellExpr::mom)) {
                 const long long r = cell / nx, c = cell % nx;
                 R.error = "boundary cell (" + std::to_string(r) + "," + std::to_string(c) +
-                          ") copies a depth or momentum that is itself a boundary value; a second application would "
-                          "change it";
+                          ") copies a depth or momentum from a boundary cell in another row; the stage kernel "
+                          "cannot apply the second boundary pass to it";
                 return R;
             }
         }

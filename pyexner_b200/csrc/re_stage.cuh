@@ -221,10 +221,15 @@ __global__ void __launch_bounds__(128, PXB_STAGE_MIN_BLOCKS) re_stage_kernel(con
                 }
             }
 
-            // ================= D: first boundary application on row q = r-3
+            // ================= D: boundary passes for the hydro fields of row q = r-3
+            // The first pass maps pre-boundary values (HF, input z_b / G) of the donors; the
+            // stored h, hu, hv are the second pass, which maps first-pass values: a donor in
+            // the same row contributes its first-pass value, a donor in another row is never
+            // a hydro boundary cell (checked at plan creation), so its value is HF.
             const int q = r - 3;
             const bool rowD = S || ((q >= L0) && (q < L1));
             T hbh = hf3h, hbu = hf3u, hbv = hf3v, zb1 = zin3, gb1 = gin3;
+            T sbh = hf3h, sbu = hf3u, sbv = hf3v;
             if (rowD && (bc_strip || (bc_rows && (q == 0 || q == ny - 1)))) {
                 const int slot = colok ? ring_slot(q, c, ny, nx) : -1;
                 unsigned flags = 0;
@@ -238,18 +243,39 @@ __global__ void __launch_bounds__(128, PXB_STAGE_MIN_BLOCKS) re_stage_kernel(con
                     m0 = T(rc.m[0]); m1 = T(rc.m[1]); m2c = T(rc.m[2]); m3 = T(rc.m[3]);
                 }
                 if (__any_sync(FULL, flags != 0)) {
-                    const T vh = __shfl_sync(FULL, pick_row(hdy, hf4h, hf3h, hf2h), lane + hdx);
-                    const T vu = __shfl_sync(FULL, pick_row(mdy, hf4u, hf3u, hf2u), lane + mdx);
-                    const T vv = __shfl_sync(FULL, pick_row(mdy, hf4v, hf3v, hf2v), lane + mdx);
-                    const T vz = __shfl_sync(FULL, pick_row(zdy, zin4, zin3, zin2), lane + zdx);
-                    const T vg = MPM ? T(0) : __shfl_sync(FULL, pick_row(gdy, gin4, gin3, gin2), lane + gdx);
+                    // donor value at (row q+dy, column c+dx); the row is chosen by the receiver
+                    auto fetch = [&](int dy, int dx_, T above, T mid, T below) {
+                        const T va = __shfl_sync(FULL, above, lane + dx_);
+                        const T vm = __shfl_sync(FULL, mid, lane + dx_);
+                        const T vb = __shfl_sync(FULL, below, lane + dx_);
+                        return pick_row(dy, va, vm, vb);
+                    };
+                    const T vh = fetch(hdy, hdx, hf4h, hf3h, hf2h);
+                    const T vu = fetch(mdy, mdx, hf4u, hf3u, hf2u);
+                    const T vv = fetch(mdy, mdx, hf4v, hf3v, hf2v);
+                    const T vz = fetch(zdy, zdx, zin4, zin3, zin2);
                     if (flags & 1u) hbh = vh;
                     if (flags & 2u) {
                         if (flags & 4u) { hbu = m0; hbv = m1; }
                         else { hbu = m0 * vu + m1 * vv; hbv = m2c * vu + m3 * vv; }
                     }
                     if (flags & 8u) zb1 = vz;
-                    if (!MPM && (flags & 16u)) gb1 = vg;
+                    if (!MPM) {
+                        const T vg = fetch(gdy, gdx, gin4, gin3, gin2);
+                        if (flags & 16u) gb1 = vg;
+                    }
+                    // second pass
+                    const T wh = fetch(hdy, hdx, hf4h, hbh, hf2h);
+                    const T wu = fetch(mdy, mdx, hf4u, hbu, hf2u);
+                    const T wv = fetch(mdy, mdx, hf4v, hbv, hf2v);
+                    sbh = hbh;
+                    sbu = hbu;
+                    sbv = hbv;
+                    if (flags & 1u) sbh = wh;
+                    if ((flags & 2u) && !(flags & 4u)) {
+                        sbu = m0 * wu + m1 * wv;
+                        sbv = m2c * wu + m3 * wv;
+                    }
                 }
             }
 
@@ -300,10 +326,12 @@ __global__ void __launch_bounds__(128, PXB_STAGE_MIN_BLOCKS) re_stage_kernel(con
                     zdy = rc.zb_dy; zdx = rc.zb_dx; gdy = rc.g_dy; gdx = rc.g_dx;
                 }
                 if (__any_sync(FULL, (flags & 24u) != 0)) {
-                    const T vz = __shfl_sync(FULL, pick_row(zdy, zbp6, zbp5, zbp4), lane + zdx);
-                    const T vg = __shfl_sync(FULL, pick_row(gdy, gg6, gg5, gg4), lane + gdx);
-                    if (flags & 8u) zfin = vz;
-                    if (flags & 16u) gfin = vg;
+                    const T z6 = __shfl_sync(FULL, zbp6, lane + zdx), z5 = __shfl_sync(FULL, zbp5, lane + zdx);
+                    const T z4 = __shfl_sync(FULL, zbp4, lane + zdx);
+                    const T g6 = __shfl_sync(FULL, gg6, lane + gdx), g5 = __shfl_sync(FULL, gg5, lane + gdx);
+                    const T g4 = __shfl_sync(FULL, gg4, lane + gdx);
+                    if (flags & 8u) zfin = pick_row(zdy, z6, z5, z4);
+                    if (flags & 16u) gfin = pick_row(gdy, g6, g5, g4);
                 }
             }
             if (rowG && p >= R0 && p < R1 && out_col) {
@@ -318,7 +346,7 @@ __global__ void __launch_bounds__(128, PXB_STAGE_MIN_BLOCKS) re_stage_kernel(con
             }
             if (rowD && q >= R0 && q < R1 && out_col) {
                 const unsigned i = (unsigned)q * upitch + (unsigned)c;
-                T oh = hbh, ou = hbu, ov = hbv;
+                T oh = sbh, ou = sbu, ov = sbv;
                 if (AVG) {
                     oh = T(0.5) * a.ah[i] + T(0.5) * oh;
                     ou = T(0.5) * a.ahu[i] + T(0.5) * ou;

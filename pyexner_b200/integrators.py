@@ -108,6 +108,15 @@ def _ssprk2_step(bundle, st, t, dt, mask, cfg):
 
 
 def _run_time_loop(state, config, io, mesh, b_mask, ssprk2):
+    """forwardeuler.py:51-132 on one device, with the time bookkeeping on the host.
+
+    Inner window (the reference's device ``while_loop``, :32-49, :80): while
+    ``time + dt_prev < target - TOL`` take a step with a fresh dt, where target is the
+    next output time (capped at end_time) and dt_prev the last dt taken.  Then the
+    window close (:85-117): a fresh dt; if it reaches the target a probe step of
+    ``target - time`` is written out (not committed); the full step is always committed.
+    SSPRK2 uses the same windows with two-stage steps.
+    """
     bundle = config.solver_bundle
     cfg = config.solver_config
     mask = bundle.mask_fn(state, cfg.mpi_handler, b_mask)
@@ -116,31 +125,28 @@ def _run_time_loop(state, config, io, mesh, b_mask, ssprk2):
         run_steps(state, mask, cfg, "SSPRK2" if ssprk2 else "FE", config.n_steps, config.cfl)
         check_state(state, mask, cfg)
         return state
+
+    def step(st, t, dt):
+        return _ssprk2_step(bundle, st, t, dt, mask, cfg) if ssprk2 else bundle.step_fn(st, t, dt, mask, cfg)
+
+    def target_of(t):
+        return min((int(t / config.out_freq) + 1) * config.out_freq, config.end_time)
+
     if io is not None:
         io.write_state(state, mesh, mask[0])
-    time = 0.0
-    num_out = 0
+    time, dt = 0.0, 0.0
     while time < config.end_time - TIMESTEP_TOL:
+        while time + dt < target_of(time) - TIMESTEP_TOL:
+            dt = float(bundle.compute_dt_fn(state, config.cfl, mask, cfg))
+            state = step(state, time, dt)
+            time += dt
         dt = float(bundle.compute_dt_fn(state, config.cfl, mask, cfg))
-        next_out = (int(time / config.out_freq) + 1) * config.out_freq
-        target = min(next_out, config.end_time)
+        target = target_of(time)
         if time + dt >= target - TIMESTEP_TOL:
-            if ssprk2:
-                # SSPRK2.py:222-225: the last step of a window lands on the target
-                dt = target - time
-            else:
-                # forwardeuler.py:93-109: probe step to the target for output only
-                probe = bundle.step_fn(state, time, target - time, mask, cfg)
-                if io is not None:
-                    io.write_state(probe, mesh, mask[0])
-                num_out += 1
-        if ssprk2:
-            state = _ssprk2_step(bundle, state, time, dt, mask, cfg)
-            if io is not None and abs((time + dt) - target) < TIMESTEP_TOL:
-                io.write_state(state, mesh, mask[0])
-                num_out += 1
-        else:
-            state = bundle.step_fn(state, time, dt, mask, cfg)
+            probe = step(state, time, target - time)
+            if io is not None:
+                io.write_state(probe, mesh, mask[0])
+        state = step(state, time, dt)
         time += dt
     check_state(state, mask, cfg)
     return state

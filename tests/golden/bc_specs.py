@@ -96,7 +96,19 @@ def partial_nodata(ny, nx):
     }
 
 
+def refl_self(ny, nx):
+    """Reflective walls whose y-normals point into the grid, as in the reference's
+    dam-break inputs (ascending y in the file): the donor clips to the cell itself."""
+    return {
+        "outlet1": _b("Reflective", left(ny, nx), [-1.0, 0.0]),
+        "outlet2": _b("Reflective", right(ny, nx), [1.0, 0.0]),
+        "outlet3": _b("Reflective", top(ny, nx), [0.0, -1.0]),
+        "outlet4": _b("Reflective", bottom(ny, nx), [0.0, 1.0]),
+    }
+
+
 BC_SPECS = {
+    "refl_self": refl_self,
     "trans_x_refl_y": trans_x_refl_y,
     "refl_first": refl_first,
     "refl_all": refl_all,

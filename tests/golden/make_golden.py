@@ -141,6 +141,7 @@ CASES = [
     ("const_fast_influx", (10, 15), "fast", "influx_left", dict(grass_factor=0.005)),
     ("const_wetdry_nodata", (12, 12), "wetdry", "partial_nodata", dict(grass_factor=0.01)),
     ("mpm1_fast_reflfirst", (11, 12), "fast", "refl_first", dict(grass_factor="MPM", bulk_porosity=0.42, sediments=SEDS_MPM["one"])),
+    ("const_fast_selfrefl", (12, 14), "fast", "refl_self", dict(grass_factor=0.005)),
 ]
 
 DX = 0.1

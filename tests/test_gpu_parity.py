@@ -86,6 +86,7 @@ def test_roe_exner_golden(request, case, dtype):
     ((64, 55), 7, "wetdry", "partial_nodata", False),
     ((40, 29), 5, "fast", "refl_first", True),
     ((37, 30), 6, "smooth", "trans_x_refl_y", True),
+    ((66, 58), 11, "fast", "refl_self", True),
 ])
 def test_roe_exner_strips_and_bands(shape, band_rows, regime, bc, mpm):
     """Grids spanning several warp strips and row bands, checked against the oracle."""
