@@ -145,6 +145,24 @@ class ClockSampler:
                 "reasons": sorted(self.reasons), "samples": len(self.sm)}
 
 
+def max_over_ranks(sec, world, device):
+    """The timed interval of the slowest rank (replicas: one all-reduce of the timing, no
+    data-path collective)."""
+    if world <= 1:
+        return float(sec)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(sec)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t)
+
+
+def replica_throughput(world, cells, steps, sec):
+    """Whole-job cell-updates/s: every rank advances its own replica of ``cells`` cells."""
+    return world * cells * steps / sec
+
+
 def build_case(n, dtype, device):
     import torch
 
@@ -405,11 +423,8 @@ def main():
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         sec, b = timed_device_loop(st, mask, cfg, args.steps, args.warmup, flush)
-    t = torch.tensor([sec], device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    sec = float(t)
-    value = world * ncell * args.steps / sec
+    sec = max_over_ranks(sec, world, "cuda")
+    value = replica_throughput(world, ncell, args.steps, sec)
     kt = kernel_breakdown(st, b, mask, cfg, max(3, args.steps // 2), flush)
     hbm, peak_kind = peaks()
     esz = 4
