@@ -231,10 +231,10 @@ def kernel_breakdown(st, b, mask, cfg, steps, flush):
         _lib.call("pxb_re_cfl", plan.handle, ctypes.byref(A), 0.5, ctypes.c_void_p(dt.data_ptr()), _stream())
         ev[1].record(stream)
         _lib.call("pxb_re_stage", plan.handle, ctypes.byref(A), ctypes.byref(B1), None,
-                  ctypes.c_void_p(dt.data_ptr()), _stream())
+                  ctypes.c_void_p(dt.data_ptr()), 0.0, _stream())
         ev[2].record(stream)
         _lib.call("pxb_re_stage", plan.handle, ctypes.byref(B2), ctypes.byref(A), ctypes.byref(A),
-                  ctypes.c_void_p(dt.data_ptr()), _stream())
+                  ctypes.c_void_p(dt.data_ptr()), 0.0, _stream())
         ev[3].record(stream)
         ev[3].synchronize()
         acc["cfl"] += ev[0].elapsed_time(ev[1]) / 1e3

@@ -38,7 +38,7 @@ extern "C" {
 #define PXB_ERR_ARG 1        /* bad argument (null pointer, size, dtype, layout)      */
 #define PXB_ERR_CUDA 2       /* a CUDA call failed                                     */
 #define PXB_ERR_NONFINITE 3  /* the device flagged a non-finite dt or state value      */
-#define PXB_ERR_UNSUPPORTED 4/* boundary layout the fused stage kernel does not cover */
+#define PXB_ERR_UNSUPPORTED 4/* boundary layout the requested stage path does not cover */
 
 #define PXB_F32 0
 #define PXB_F64 1
@@ -53,10 +53,27 @@ extern "C" {
 #define PXB_BC_RE_CONSTANTINFLUX 4   /* "Roe Exner ConstantInflux"  roeexner_constantinflux.py:18-48  */
 #define PXB_BC_ROE_REFLECTIVE 5      /* "Roe Reflective"            roe_reflective.py:18-44           */
 #define PXB_BC_ROE_TRANSMISSIVE 6    /* "Roe Transmissive"          roe_transmissive.py:17-43         */
+#define PXB_BC_RE_CONSTANTOUTFLUX 7  /* "Roe Exner ConstantOutflux" roeexner_constantoutflux.py:18-73 */
+#define PXB_BC_RE_BERTHON 8          /* "Roe Exner Berthon"         roeexner_berthon.py:19-56         */
+#define PXB_BC_RE_NORMALFLOWDEPTH 9  /* "Roe Exner NormalFlowDepth" roeexner_normalflowdepth.py:19-51 */
+#define PXB_BC_RE_STEEPFALL 10       /* "Roe Exner SteepFall"       roeexner_steepfall.py:17-26       */
+#define PXB_BC_RE_ZEROMOMENTUM 11    /* "Roe Exner ZeroMomentum"    roeexner_zeromomentum.py:16-31    */
+
+/* Stage paths of a Roe-Exner plan (pxb_re_config.stage_path). */
+#define PXB_PATH_AUTO 0     /* fused when the boundary layout allows it, else general          */
+#define PXB_PATH_FUSED 1    /* one fused kernel per stage; ring layouts of kinds 1-4 only       */
+#define PXB_PATH_GENERAL 2  /* cell-parallel kernel chain; any handler layout and kind          */
 
 /* One boundary handler: cells by (flat row*pitch+col) index, donors alike.
  * Replaces a handler object built by BoundaryManager (boundary_registry.py:132-171)
- * with the index maps of compute_reflective_indices (boundary_registry.py:61-82). */
+ * with the index maps of compute_reflective_indices (boundary_registry.py:61-82).
+ * ZeroMomentum handlers carry the cells of their mask and use each cell as its own donor.
+ * values: the YAML values as the reference parses them (float32, NaN allowed,
+ * boundary_registry.py:107-110), zero-padded to 8:
+ *   ConstantOutflux  [q, nx, ny]                  Newton depth on the outgoing invariant
+ *   Berthon          [q, A, alpha, beta, gamma, x] z_b = -alpha*t + zb0(q, A, alpha, beta, gamma, x)
+ *   NormalFlowDepth  [q, A, alpha, beta, gamma, x] as Berthon, and h = q/u
+ *   ZeroMomentum     [h, hu, hv, z]               hu = values[1]*nx, hv = values[1]*ny (NaN: keep) */
 typedef struct pxb_bc_handler {
     int32_t kind;
     int32_t count;          /* number of (boundary, donor) pairs            */
@@ -64,6 +81,7 @@ typedef struct pxb_bc_handler {
     const int64_t* donors;  /* host array, `count` donor (interior) cells   */
     double nx, ny;          /* outward normal as given in the YAML          */
     double hu_const, hv_const; /* ConstantInflux: float32(values[0]*values[1]), float32(values[0]*values[2]) */
+    double values[8];
 } pxb_bc_handler;
 
 /* Per ring cell, the boundary result after all handlers, as a function of the
@@ -122,6 +140,7 @@ typedef struct pxb_re_config {
     const pxb_bc_handler* handlers; /* in YAML order; resolved into ring recipes at plan creation */
     int32_t nhandlers;
     int32_t band_rows;              /* rows per warp band of the stage kernel; 0 = automatic   */
+    int32_t stage_path;             /* PXB_PATH_AUTO / _FUSED / _GENERAL                       */
 } pxb_re_config;
 
 /* --- Roe-Exner ------------------------------------------------------------------ */
@@ -131,23 +150,31 @@ int pxb_re_plan_destroy(pxb_re_plan* plan);
 /* init_fn_roeexner (roe_exner_solver.py:58-78): n_b, G, then the handlers at t = 0, in place. */
 int pxb_re_init(pxb_re_plan* plan, const pxb_re_fields* f, void* stream);
 
+/* The stage path the plan resolved to: PXB_PATH_FUSED or PXB_PATH_GENERAL. */
+int pxb_re_plan_path(const pxb_re_plan* plan);
+
 /* compute_dt_roeexner (roe_exner_solver.py:118-122): dt = max(cfl * min_faces dt_face, 1e-6)
  * written to dt_dev (one element of the plan dtype, device memory). */
 int pxb_re_cfl(pxb_re_plan* plan, const pxb_re_fields* f, double cfl, void* dt_dev, void* stream);
 
 /* step_fn_roeexner (roe_exner_solver.py:80-116): one stage from `in` to `out` with the
- * device scalar dt.  If `avg` is not NULL the result is 0.5*avg + 0.5*stage(in) on
- * h, hu, hv, z_b, G (the SSPRK2 combination, SSPRK2.py:40); out may alias avg, never in.
- * out->G may be NULL when the caller does not need G (it is recomputed in MPM mode). */
+ * device scalar dt at simulation time `time` (read by time-dependent handlers).  If `avg`
+ * is not NULL the result is 0.5*avg + 0.5*stage(in) on h, hu, hv, z_b, G (the SSPRK2
+ * combination, SSPRK2.py:40); out may alias avg, never in.  out->G may be NULL when the
+ * caller does not need G (it is recomputed in MPM mode).  The general path also carries
+ * n through the handlers: it writes out->n when set (averaged with avg->n when both are
+ * set); the fused path leaves n alone (its plans only accept layouts that keep n fixed). */
 int pxb_re_stage(pxb_re_plan* plan, const pxb_re_fields* in, const pxb_re_fields* out,
-                 const pxb_re_fields* avg, const void* dt_dev, void* stream);
+                 const pxb_re_fields* avg, const void* dt_dev, double time, void* stream);
 
 /* A fixed number of integrator steps (forwardeuler.py:37-49 / SSPRK2.py:30-51 without
- * output probes).  The state starts and ends in `a`; `b` is scratch state of the same
- * layout (h, hu, hv, z_b, G are written).  dt_log: device array of nsteps dts or NULL.
- * The steps are captured once into a CUDA graph and replayed. */
+ * output probes), starting at simulation time t0; the time of each step (the sum of the
+ * dts before it, in float64) is kept on the device.  The state starts and ends in `a`;
+ * `b` is scratch state of the same layout (h, hu, hv, z_b, G are written; n too on the
+ * general path, which needs b->n distinct from a->n).  dt_log: device array of nsteps
+ * dts or NULL.  The steps are captured once into a CUDA graph and replayed. */
 int pxb_re_run(pxb_re_plan* plan, const pxb_re_fields* a, const pxb_re_fields* b, int32_t nsteps,
-               int32_t scheme, double cfl, void* dt_log, void* stream);
+               int32_t scheme, double cfl, double t0, void* dt_log, void* stream);
 
 /* Device error word of the plan (non-finite dt or state seen by a kernel): reads it
  * (synchronising `stream`), clears it, returns PXB_OK or PXB_ERR_NONFINITE. */

@@ -57,14 +57,20 @@ class Handler:
         self.normal = np.asarray(normal, dtype=np.float64)
         # the reference parses values into a float32 array (boundary_registry.py:107-110)
         self.values = np.asarray(values, dtype=np.float32)
-        self.b, self.i = index_maps(mask, normal)
+        if kind == "Roe Exner ZeroMomentum":
+            # a mask handler without index maps (boundary_registry.py:164-169): list its cells
+            c = np.argwhere(mask)
+            self.b = self.i = (c[:, 0], c[:, 1])
+        else:
+            self.b, self.i = index_maps(mask, normal)
 
-    def apply(self, st):
+    def apply(self, st, time=0.0):
         st = dict(st)
         by, bx = self.b
         iy, ix = self.i
         nx, ny = self.normal
         k = self.kind
+        v = self.values
         if k == "Roe Exner Reflective":  # roeexner_reflective.py:17-63
             hu_i = st["hu"][iy, ix]
             hv_i = st["hv"][iy, ix]
@@ -96,6 +102,39 @@ class Handler:
             }
         elif k == "Roe Transmissive":  # roe_transmissive.py:17-43
             new = {f: st[f][iy, ix] for f in ("h", "z", "n", "hu", "hv")}
+        elif k == "Roe Exner ConstantOutflux":  # roeexner_constantoutflux.py:18-59
+            q, vx, vy = v[0], v[1], v[2]
+            h_i = np.maximum(st["h"][iy, ix], 1e-8)
+            u_i = st["hu"][iy, ix] / h_i
+            v_i = st["hv"][iy, ix] / h_i
+            un_i = u_i * vx + v_i * vy
+            rp = un_i + 2.0 * np.sqrt(9.81 * h_i)
+            h = h_i
+            for _ in range(5):  # Newton on the outgoing Riemann invariant
+                h = np.maximum(h, 1e-8)
+                c = np.sqrt(9.81 * h)
+                f = q / h + 2.0 * c - rp
+                df = -q / (h * h) + 9.81 / np.maximum(c, 1e-8)
+                h = np.maximum(h - f / df, 1e-8)
+            new = {"h": h, "hu": np.float64(q * vx), "hv": np.float64(q * vy)}
+        elif k in ("Roe Exner Berthon", "Roe Exner NormalFlowDepth"):
+            # roeexner_berthon.py:19-56, roeexner_normalflowdepth.py:19-51 (float32 values)
+            q, A, alpha, beta, gamma, x = v[0], v[1], v[2], v[3], v[4], v[5]
+            u = np.power((alpha * x + beta) / A, np.float32(1.0 / 3.0))
+            zb0 = -(u * (u * u) + 2.0 * 9.81 * q) / (2.0 * 9.81 * np.maximum(u, np.float32(1e-12))) + gamma
+            zb = -alpha * np.float32(time) + zb0
+            new = {"z_b": np.float64(zb)}
+            if k == "Roe Exner NormalFlowDepth":
+                new.update(h=np.float64(q / u), hu=st["hu"][iy, ix], hv=st["hv"][iy, ix])
+        elif k == "Roe Exner SteepFall":  # roeexner_steepfall.py:17-26
+            new = {"z_b": st["z_b"][iy, ix] - 1}
+        elif k == "Roe Exner ZeroMomentum":  # roeexner_zeromomentum.py:16-31 (mask, no donors)
+            m = self.mask
+            hu_val = v[1] * self.normal[0]
+            hv_val = v[1] * self.normal[1]
+            st["hu"] = np.where(m, st["hu"] if np.isnan(hu_val) else hu_val, st["hu"])
+            st["hv"] = np.where(m, st["hv"] if np.isnan(hv_val) else hv_val, st["hv"])
+            return st
         else:
             raise KeyError(f"boundary type '{k}' is not on the oracle's path")
         for f, v in new.items():
@@ -118,9 +157,9 @@ class Boundaries:
             vals = [np.nan if str(v).lower() == "nan" else float(v) for v in spec.get("values", [])]
             self.handlers.append(Handler(kind, m, spec["normal"], vals))
 
-    def apply(self, st):
+    def apply(self, st, time=0.0):
         for hd in self.handlers:
-            st = hd.apply(st)
+            st = hd.apply(st, time)
         return st
 
 

@@ -164,7 +164,7 @@ static double grass(const oc_case* C, double h, double hu, double hv, int m0, do
         double th = (np_ * np_ * vel2) / ((s - 1.0) * d50 * cbrt(hc));
         th = maxd(th, 0.0);
         const double dth = maxd(th - thc, 0.0);
-        const double g1 = pow(np_, 3.0) * sqrt(G_ACC) / ((s - 1.0) * sqrt(hc));
+        const double g1 = np_ * (np_ * np_) * sqrt(G_ACC) / ((s - 1.0) * sqrt(hc));
         const double g2 = 8.0 * sqrt(dth) / (pow(th, 1.5) + 1e-5);
         const double c = frac * g1 * g2 * dth;
         G = k == 0 ? c : G + c;
@@ -212,7 +212,7 @@ static double face_dt(const double* si, const double* sj, int yf, double dx) {
     } else {
         const double b = -2 * ut, c = (1 + at) * (ct * ct) - ut * ut, d = -(ct * ct) * at * ut;
         const double p = (-3 * c - b * b) / 3.0;
-        const double q = (2 * pow(b, 3.0) - (-9 * b) * c + 27 * d) / -27.0;
+        const double q = (2 * (b * (b * b)) - (-9 * b) * c + 27 * d) / -27.0;
         double x = (3 * q) / (2 * p) * sqrt(-3 / p);
         x = x < -1.0 ? -1.0 : (x > 1.0 ? 1.0 : x);
         const double th = acos(x), sq = 2 * sqrt(-p / 3), shift = -b / -3.0;
@@ -252,7 +252,8 @@ double oc_re_cfl(const oc_case* C, const oc_state* s, double cfl) {
     return maxd(cfl * best, 1e-6);
 }
 
-/* one stage: s -> o (o's planes are overwritten; z, n, nb are shared and read only) */
+/* one stage: s -> o (o's planes are overwritten, n included: boundary handlers write it;
+   z and nb are shared and read only) */
 void oc_re_stage(const oc_case* C, const oc_state* s, oc_state* o, double dt, double* work) {
     const int ny = C->ny, nx = C->nx;
     const int64_t N = (int64_t)ny * nx;
@@ -304,6 +305,7 @@ void oc_re_stage(const oc_case* C, const oc_state* s, oc_state* o, double dt, do
             o->hv[i] = s->hv[i] - dt * f[2] / dx;
             o->zb[i] = s->zb[i];
             o->G[i] = s->G[i];
+            o->n[i] = s->n[i];
         }
     /* momentum corrections on the interior (roe_exner.py:14-62), in place: they read h only */
 #pragma omp parallel for schedule(static)
@@ -373,7 +375,7 @@ void oc_re_init(const oc_case* C, oc_state* s) {
 /* nsteps Forward-Euler (scheme 0) or SSPRK2 (scheme 1) steps in place; dts[nsteps] out */
 int oc_re_run(const oc_case* C, oc_state* s, int nsteps, int scheme, double cfl, double* dts) {
     const int64_t N = (int64_t)C->ny * C->nx;
-    double* buf = (double*)malloc(sizeof(double) * (size_t)(N * 5 + N * 12));
+    double* buf = (double*)malloc(sizeof(double) * (size_t)(N * 6 + N * 12));
     if (!buf) return 1;
     oc_state a = *s, b = *s;
     b.h = buf;
@@ -381,19 +383,21 @@ int oc_re_run(const oc_case* C, oc_state* s, int nsteps, int scheme, double cfl,
     b.hv = buf + 2 * N;
     b.zb = buf + 3 * N;
     b.G = buf + 4 * N;
-    double* work = buf + 5 * N;
+    b.n = buf + 5 * N;
+    double* work = buf + 6 * N;
     for (int k = 0; k < nsteps; ++k) {
         const double dt = oc_re_cfl(C, &a, cfl);
         if (dts) dts[k] = dt;
         oc_re_stage(C, &a, &b, dt, work);
         if (scheme == 1) {
             oc_state c2 = b;
-            double* tmp = (double*)malloc(sizeof(double) * (size_t)(N * 5));
+            double* tmp = (double*)malloc(sizeof(double) * (size_t)(N * 6));
             c2.h = tmp;
             c2.hu = tmp + N;
             c2.hv = tmp + 2 * N;
             c2.zb = tmp + 3 * N;
             c2.G = tmp + 4 * N;
+            c2.n = tmp + 5 * N;
             oc_re_stage(C, &b, &c2, dt, work);
 #pragma omp parallel for schedule(static)
             for (int64_t i = 0; i < N; ++i) {
@@ -402,6 +406,7 @@ int oc_re_run(const oc_case* C, oc_state* s, int nsteps, int scheme, double cfl,
                 a.hv[i] = 0.5 * a.hv[i] + 0.5 * c2.hv[i];
                 a.zb[i] = 0.5 * a.zb[i] + 0.5 * c2.zb[i];
                 a.G[i] = 0.5 * a.G[i] + 0.5 * c2.G[i];
+                a.n[i] = 0.5 * a.n[i] + 0.5 * c2.n[i];
             }
             free(tmp);
         } else {
@@ -410,6 +415,7 @@ int oc_re_run(const oc_case* C, oc_state* s, int nsteps, int scheme, double cfl,
             memcpy(a.hv, b.hv, sizeof(double) * (size_t)N);
             memcpy(a.zb, b.zb, sizeof(double) * (size_t)N);
             memcpy(a.G, b.G, sizeof(double) * (size_t)N);
+            memcpy(a.n, b.n, sizeof(double) * (size_t)N);
         }
     }
     free(buf);

@@ -23,17 +23,21 @@ def _avg(a, b, fields):
     return out
 
 
-def run_roe_exner(st, mask, bcs, mpm, dx, cfl, nsteps, scheme):
+def run_roe_exner(st, mask, bcs, mpm, dx, cfl, nsteps, scheme, t0=0.0):
+    """Fixed-step loop; the time argument of every stage is the time at the start of
+    its step (SSPRK2.py:36-37 passes the same time to both stages)."""
     dts = []
+    t = t0
     for _ in range(nsteps):
         dt = _re.compute_dt(st, cfl, dx, mask[0])
         if scheme == "SSPRK2":
-            s1 = _re.stage(st, dt, dx, mask, bcs, mpm)
-            s2 = _re.stage(s1, dt, dx, mask, bcs, mpm)
+            s1 = _re.stage(st, dt, dx, mask, bcs, mpm, t)
+            s2 = _re.stage(s1, dt, dx, mask, bcs, mpm, t)
             st = _avg(st, s2, _re.STATE_FIELDS)
         else:
-            st = _re.stage(st, dt, dx, mask, bcs, mpm)
+            st = _re.stage(st, dt, dx, mask, bcs, mpm, t)
         dts.append(float(dt))
+        t = t + float(dt)
     return st, np.array(dts)
 
 

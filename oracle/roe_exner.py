@@ -211,7 +211,8 @@ def compute_G_mpm(h, hu, hv, seds, mask0):
         theta = np.maximum(theta, 0.0)
         dtheta = np.maximum(theta - theta_c, 0.0)
         sqrt_h = np.sqrt(h)
-        g1 = n_p**3 * np.sqrt(G_ACC) / ((s - 1.0) * sqrt_h)
+        # n_p**3 and b**3 below are jax integer_pow: repeated multiplication, not pow()
+        g1 = n_p * (n_p * n_p) * np.sqrt(G_ACC) / ((s - 1.0) * sqrt_h)
         g2 = 8.0 * np.sqrt(dtheta) / (theta**1.5 + 1e-5)
         G = np.sum(frac * g1 * g2 * dtheta, axis=0)
         G = G / (1.0 - porosity.mean())
@@ -297,7 +298,7 @@ def _lambda_cubic(ut, at, ct):
     d = -ct**2 * at * ut
     with np.errstate(all="ignore"):
         p = (3 * a * c - b**2) / (3 * a**2)
-        q = (2 * b**3 - 9 * a * b * c + 27 * a**2 * d) / (27 * a**3)
+        q = (2 * (b * (b * b)) - 9 * a * b * c + 27 * a**2 * d) / (27 * a**3)
         cos_t = np.clip((3 * q) / (2 * p) * np.sqrt(-3 / p), -1.0, 1.0)
         theta = np.arccos(cos_t)
         sq = 2 * np.sqrt(-p / 3)
@@ -365,7 +366,7 @@ def init(st, mask, bcs, mpm):
     return bcs.apply(st)
 
 
-def stage(st, dt, dx, mask, bcs, mpm):
+def stage(st, dt, dx, mask, bcs, mpm, time=0.0):
     """``step_fn_roeexner`` on one rank (roe_exner_solver.py:80-116).
 
     hydro (a5) -> momentum corrections (a6) -> BCs (a7) -> G (a8) -> Exner (a9) -> BCs.
@@ -376,10 +377,10 @@ def stage(st, dt, dx, mask, bcs, mpm):
     h, hu, hv = hydro_update(st, dt, dx, mask)
     hu, hv = momentum_corrections(h, hu, hv, st["z"], st["z_b"], mask[0])
     st.update(h=h, hu=hu, hv=hv)
-    st = bcs.apply(st)
+    st = bcs.apply(st, time)
     st["G"] = compute_G(st, mask[0], mpm)
     st["z_b"] = exner_update(st, dt, dx, mask[0])
-    return bcs.apply(st)
+    return bcs.apply(st, time)
 
 
 def hydro_and_corrections(st, dt, dx, mask):

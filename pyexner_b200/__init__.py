@@ -4,6 +4,7 @@ The public surface mirrors PyExner's (src/PyExner/__init__.py): ``run_driver`` a
 state / solver / integrator registries.  Compute goes through ``libpyexner_b200.so``
 (include/pyexner_b200.h); build it with ``python -m pyexner_b200.build``.
 """
+from ._lib import PxbError
 from .boundaries import BoundaryManager
 from .integrators import (
     INTEGRATOR_REGISTRY,
@@ -35,6 +36,7 @@ __all__ = [
     "create_integrator_bundle",
     "register_integrator_bundle",
     "run_steps",
+    "PxbError",
 ]
 
 

@@ -17,6 +17,7 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "pyexner_b200.h")
 OK, ERR_ARG, ERR_CUDA, ERR_NONFINITE, ERR_UNSUPPORTED = 0, 1, 2, 3, 4
 F32, F64 = 0, 1
 FE, SSPRK2 = 0, 1
+PATH_AUTO, PATH_FUSED, PATH_GENERAL = 0, 1, 2
 BC_KINDS = {
     "Roe Exner Reflective": 1,
     "Roe Exner Transmissive": 2,
@@ -24,6 +25,11 @@ BC_KINDS = {
     "Roe Exner ConstantInflux": 4,
     "Roe Reflective": 5,
     "Roe Transmissive": 6,
+    "Roe Exner ConstantOutflux": 7,
+    "Roe Exner Berthon": 8,
+    "Roe Exner NormalFlowDepth": 9,
+    "Roe Exner SteepFall": 10,
+    "Roe Exner ZeroMomentum": 11,
 }
 
 
@@ -37,6 +43,7 @@ class BcHandler(ctypes.Structure):
         ("ny", c_double),
         ("hu_const", c_double),
         ("hv_const", c_double),
+        ("values", c_double * 8),
     ]
 
 
@@ -62,6 +69,7 @@ class REConfig(ctypes.Structure):
         ("handlers", POINTER(BcHandler)),
         ("nhandlers", c_int32),
         ("band_rows", c_int32),
+        ("stage_path", c_int32),
     ]
 
 
@@ -90,9 +98,12 @@ SIGNATURES = {
     "pxb_re_plan_create": [POINTER(REConfig), POINTER(c_void_p)],
     "pxb_re_plan_destroy": [c_void_p],
     "pxb_re_init": [c_void_p, POINTER(REFields), c_void_p],
+    "pxb_re_plan_path": [c_void_p],
     "pxb_re_cfl": [c_void_p, POINTER(REFields), c_double, c_void_p, c_void_p],
-    "pxb_re_stage": [c_void_p, POINTER(REFields), POINTER(REFields), POINTER(REFields), c_void_p, c_void_p],
-    "pxb_re_run": [c_void_p, POINTER(REFields), POINTER(REFields), c_int32, c_int32, c_double, c_void_p, c_void_p],
+    "pxb_re_stage": [c_void_p, POINTER(REFields), POINTER(REFields), POINTER(REFields), c_void_p, c_double,
+                     c_void_p],
+    "pxb_re_run": [c_void_p, POINTER(REFields), POINTER(REFields), c_int32, c_int32, c_double, c_double, c_void_p,
+                   c_void_p],
     "pxb_re_check": [c_void_p, c_void_p],
     "pxb_roe_plan_create": [POINTER(RoeConfig), POINTER(c_void_p)],
     "pxb_roe_plan_destroy": [c_void_p],

@@ -5,7 +5,8 @@ each YAML ``boundaries`` entry names a polygon, a type, an outward normal and va
 the polygon selects cells by even-odd ray casting on the cell centres (:19-59) and
 every selected cell takes its donor one step against the normal (:61-82).  The handler
 list is handed to the C ABI in YAML order; the library resolves it into per-ring-cell
-recipes that the stage kernels apply in registers.
+recipes that the fused stage kernel applies in registers, or applies the handlers one
+after another on the general stage path.
 """
 from __future__ import annotations
 
@@ -75,7 +76,12 @@ class BoundaryManager:
             vals = np.array([np.nan if str(v).lower() == "nan" else float(v) for v in spec.get("values", [])],
                             dtype=np.float32)
             normal = [float(v) for v in spec["normal"]]
-            (by, bx), (iy, ix) = index_maps(m, normal)
+            if kind == "Roe Exner ZeroMomentum":
+                # mask handler (roeexner_zeromomentum.py:16-31): every mask cell is its own donor
+                b = np.argwhere(m)
+                (by, bx), (iy, ix) = (b[:, 0], b[:, 1]), (b[:, 0], b[:, 1])
+            else:
+                (by, bx), (iy, ix) = index_maps(m, normal)
             hu_c = hv_c = 0.0
             if kind == "Roe Exner ConstantInflux":
                 # float32 values as parsed by boundary_registry.py:107-110, product in float32
@@ -103,6 +109,9 @@ class BoundaryManager:
             arr[k].nx, arr[k].ny = hd["normal"]
             arr[k].hu_const = hd["hu_const"]
             arr[k].hv_const = hd["hv_const"]
+            vals = hd["values"][:8]
+            for j, v in enumerate(vals):
+                arr[k].values[j] = float(v)  # float32 values, NaN kept
         arr._keep = keep
         return arr, n
 

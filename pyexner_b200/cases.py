@@ -97,3 +97,54 @@ def gaussian_bed(n, dx=0.01, seed_bed=1, seed_noise=2, device=None):
     params = dict(flux_scheme="Roe Exner", integrator="SSPRK2", cfl=0.5, erosion=erosion, boundaries=bspec)
     return dict(arrs=arrs, seds=seds_matrix(erosion), dx=dx, params=params,
                 boundaries=BoundaryManager(params, X, Y), X=X, Y=Y)
+
+
+# ------------------------------------------------------------------ Berthon analytic case
+BERTHON = dict(q=1.0, A=0.005, alpha=0.005, beta=0.005, gamma=1.0)
+
+
+def berthon_exact(x, t, q=1.0, A=0.005, alpha=0.005, beta=0.005, gamma=1.0, g=9.81):
+    """Analytic steady-flow / linearly eroding bed of Berthon et al. (the reference's
+    tests/runtime/2D_const_flux/analyze_convergence.py:9-25): with a constant grass
+    factor A, u = ((alpha x + beta) / A)^(1/3), h = q / u, hu = q and
+    z_b = -alpha t - (u^3 + 2 g q) / (2 g u) + gamma, so that dz_b/dt = -alpha exactly."""
+    u = ((alpha * x + beta) / A) ** (1.0 / 3.0)
+    h = q / u
+    zb = -alpha * t - (u**3 + 2 * g * q) / (2 * g * u) + gamma
+    return h, q * np.ones_like(x), zb
+
+
+def berthon_case(dh=0.1, end_time=10.0, out_freq=1.0, integrator="Forward Euler"):
+    """Input of the reference's 2D_const_flux case (tests/runtime/2D_const_flux/
+    2D_build_num_sol.py:8-56 and input.yaml): the analytic state at t = 0 on
+    x in [0, 7], y in [0, 1] (file rows from y = 1 down to 0) with spacing dh, and the
+    run parameters: constant grass factor 0.005, ConstantInflux + Berthon bed at the
+    inlet, NormalFlowDepth at the outlet, reflective walls, CFL 0.5.
+
+    Returns (x, y, fields, params): file coordinates, float64 planes and the YAML dict
+    (without input_file / output_file)."""
+    c = BERTHON
+    x = np.arange(0.0, 7.0 + dh, dh)
+    y = np.arange(1.0, 0.0 - dh, -dh)
+    X, _ = np.meshgrid(x, y, indexing="xy")
+    h, hu, zb = berthon_exact(X, 0.0, **c)
+    zeros = np.zeros_like(h)
+    fields = dict(h=h, hu=hu, hv=zeros, z_b=zb, z=zeros, n=zeros)
+    vals = [c["q"], c["A"], c["alpha"], c["beta"], c["gamma"]]
+    params = dict(
+        end_time=end_time, out_freq=out_freq, cfl=0.5, flux_scheme="Roe Exner", integrator=integrator,
+        parNx=1, parNy=1, erosion=dict(grass_factor=0.005),
+        boundaries=dict(
+            inlet_flux=dict(type="ConstantInflux", polygon=[[0.0, 0.0], [0.05, 0.0], [0.05, 1.0], [0.0, 1.0]],
+                            values=[1.0, 1.0, 0.0], normal=[-1.0, 0.0]),
+            inlet_bed=dict(type="Berthon", polygon=[[0.0, 0.0], [0.05, 0.0], [0.05, 1.0], [0.0, 1.0]],
+                           values=vals + [0.025], normal=[-1.0, 0.0]),
+            outlet_bed=dict(type="NormalFlowDepth", polygon=[[6.95, 0.0], [7.05, 0.0], [7.05, 1.05], [6.95, 1.05]],
+                            values=vals + [6.975], normal=[1.0, 0.0]),
+            bottom=dict(type="Reflective", polygon=[[0.0, -0.05], [7.05, -0.05], [7.05, 0.05], [0.0, 0.05]],
+                        values=[0, 0, 0, 0], normal=[0.0, -1.0]),
+            top=dict(type="Reflective", polygon=[[0.0, 1.05], [7.05, 1.05], [7.05, 0.95], [0.0, 0.95]],
+                     values=[0, 0, 0, 0], normal=[0.0, 1.0]),
+        ),
+    )
+    return x, y, fields, params

@@ -5,7 +5,9 @@
 //     thread-local message;
 //   * resolve the ordered boundary handlers into per-ring-cell recipes (the symbolic
 //     equivalent of applying PyExner's handlers one after another,
-//     src/PyExner/domain/boundary_registry.py:183-187) and upload them once;
+//     src/PyExner/domain/boundary_registry.py:183-187) and upload them once; layouts that
+//     do not resolve run on the general stage path (re_general.cuh), which applies the
+//     handlers one after another on the device;
 //   * turn the sediment matrix into per-class constants;
 //   * size the warp strips / row bands of the stage and CFL kernels to the device;
 //   * capture the fixed-step integrator loops into CUDA graphs and replay them.
@@ -141,6 +143,15 @@ Resolved resolve(const pxb_bc_handler* hs, int nh, int ny, int nx, long long pit
                     setg(ne.n, get(mp, d, &CellExpr::n));
                     setg(ne.mom, get(mp, d, &CellExpr::mom));
                     break;
+                case PXB_BC_RE_CONSTANTOUTFLUX:
+                case PXB_BC_RE_BERTHON:
+                case PXB_BC_RE_NORMALFLOWDEPTH:
+                case PXB_BC_RE_STEEPFALL:
+                case PXB_BC_RE_ZEROMOMENTUM:
+                    R.error = "boundary kind " + std::to_string(H.kind) +
+                              " computes its values from the time or from donor values; it runs on the general "
+                              "stage path only";
+                    return R;
                 default:
                     R.error = "unknown boundary kind " + std::to_string(H.kind);
                     return R;
@@ -219,6 +230,19 @@ Resolved resolve(const pxb_bc_handler* hs, int nh, int ny, int nx, long long pit
                           "cannot apply the second boundary pass to it";
                 return R;
             }
+            // The fused kernel never writes n: the n left by the set-up application must be
+            // a fixed point of the handlers, i.e. no cell copies n from a cell whose own n
+            // comes from somewhere else.
+            if (e.n.set && e.n.src != cell) {
+                auto it = mp.find(e.n.src);
+                if (it != mp.end() && it->second.n.set && it->second.n.src != e.n.src) {
+                    const long long r = cell / nx, c = cell % nx;
+                    R.error = "boundary cell (" + std::to_string(r) + "," + std::to_string(c) +
+                              ") copies n from a boundary cell whose n changes with every application; the fused "
+                              "stage kernel keeps n fixed";
+                    return R;
+                }
+            }
         }
     }
     return R;
@@ -230,7 +254,33 @@ struct DevHandler {
     long long* cells = nullptr;
     long long* donors = nullptr;
     double nx = 0, ny = 0, c0 = 0, c1 = 0;
+    double q = 0, vx = 0, vy = 0, hb = 0;  // ConstantOutflux, NormalFlowDepth
+    float neg_alpha = 0, zb0 = 0;          // Berthon, NormalFlowDepth
 };
+
+// Constants of the Berthon analytic inlet / outlet, in float32 like the reference's
+// float32 values (roeexner_berthon.py:40-52, roeexner_normalflowdepth.py:34-41):
+//   u = ((alpha x + beta) / A)^(1/3),  zb0 = -(u^3 + 2 g q) / (2 g max(u, 1e-12)) + gamma,
+//   h = q / u.  u^3 is u * (u * u) (jax integer_pow); the cube root is the correctly
+// rounded float32 power, taken in double precision and rounded once.
+void berthon_constants(const double* v, DevHandler& d) {
+    const float q = (float)v[0], A = (float)v[1], alpha = (float)v[2], beta = (float)v[3];
+    const float gamma = (float)v[4], x = (float)v[5];
+    const float ax = alpha * x;
+    const float w = (ax + beta) / A;
+    const float third = 1.0f / 3.0f;
+    const float u = (float)std::pow((double)w, (double)third);
+    const float g2 = (float)(2.0 * 9.81);
+    const float u3 = u * (u * u);
+    const float num = u3 + g2 * q;
+    const float tiny = (float)1e-12;
+    const float umax = (u != u) ? u : (u < tiny ? tiny : u);  // jnp.maximum (NaN propagates)
+    const float den = g2 * umax;
+    d.zb0 = -num / den + gamma;
+    d.neg_alpha = -alpha;
+    d.hb = (double)(q / u);
+    d.q = q;
+}
 
 struct Geometry {
     int band_rows = 0, nstrips = 0, nbands = 0, grid = 0;
@@ -279,6 +329,28 @@ int upload_handlers(const pxb_bc_handler* hs, int nh, long long max_index, std::
         d.ny = H.ny;
         d.c0 = H.hu_const;
         d.c1 = H.hv_const;
+        const double* v = H.values;
+        switch (H.kind) {
+            case PXB_BC_RE_CONSTANTOUTFLUX: {  // float32 values, float32 momenta (roeexner_constantoutflux.py:29-64)
+                const float q = (float)v[0], vx = (float)v[1], vy = (float)v[2];
+                d.q = q;
+                d.vx = vx;
+                d.vy = vy;
+                d.c0 = (double)(q * vx);
+                d.c1 = (double)(q * vy);
+                break;
+            }
+            case PXB_BC_RE_BERTHON:
+            case PXB_BC_RE_NORMALFLOWDEPTH:
+                berthon_constants(v, d);
+                break;
+            case PXB_BC_RE_ZEROMOMENTUM:  // values[1] * normal (roeexner_zeromomentum.py:26-27)
+                d.c0 = (double)(float)v[1] * H.nx;
+                d.c1 = (double)(float)v[1] * H.ny;
+                break;
+            default:
+                break;
+        }
         if (H.count > 0) {
             PXB_CUDA(cudaMalloc(&d.cells, sizeof(long long) * H.count));
             PXB_CUDA(cudaMalloc(&d.donors, sizeof(long long) * H.count));
@@ -304,7 +376,7 @@ void fill_sed(pxb::SedTable<T>& S, const double* seds, int nsed) {
         S.s[k].np2 = (T)(np_ * np_);
         S.s[k].sm1d = (T)((s - 1.0) * d50);
         S.s[k].thc = (T)thc;
-        S.s[k].np3sg = (T)(std::pow(np_, 3.0) * std::sqrt(9.81));
+        S.s[k].np3sg = (T)(np_ * (np_ * np_) * std::sqrt(9.81));  // n_p**3 as jax integer_pow
         S.s[k].sm1 = (T)(s - 1.0);
         S.s[k].frac = (T)frac;
         por_sum += por;
@@ -318,7 +390,7 @@ void fill_sed(pxb::SedTable<T>& S, const double* seds, int nsed) {
         const double s = dens / 1000.0;
         const double np_ = std::pow(d50, 1.0 / 6.0) / 21.1;
         S.k_theta[k] = (T)(np_ * np_ / ((s - 1.0) * d50));
-        S.k_g1[k] = (T)(8.0 * frac * std::pow(np_, 3.0) * std::sqrt(9.81) / (s - 1.0));
+        S.k_g1[k] = (T)(8.0 * frac * (np_ * (np_ * np_)) * std::sqrt(9.81) / (s - 1.0));
     }
 }
 
@@ -365,8 +437,16 @@ struct PlanCommon {
     }
 };
 
+// Boundary kinds a plan accepts: the "Roe Exner" handlers or the "Roe" handlers.
+bool kind_ok(int kind, bool roe) {
+    if (roe) return kind == PXB_BC_ROE_REFLECTIVE || kind == PXB_BC_ROE_TRANSMISSIVE;
+    return (kind >= PXB_BC_RE_REFLECTIVE && kind <= PXB_BC_RE_CONSTANTINFLUX) ||
+           (kind >= PXB_BC_RE_CONSTANTOUTFLUX && kind <= PXB_BC_RE_ZEROMOMENTUM);
+}
+
+// want_path: PXB_PATH_AUTO / _FUSED / _GENERAL (Roe plans: fused only); path: the result.
 int common_setup(PlanCommon& P, int ny, int nx, long long pitch, int dtype, double dx, const pxb_bc_handler* hs,
-                 int nh, bool roe) {
+                 int nh, bool roe, int want_path, int& path) {
     if (ny < 3 || nx < 3) return fail(PXB_ERR_ARG, "grid must be at least 3 x 3 cells including the ring");
     if (pitch < nx) return fail(PXB_ERR_ARG, "pitch smaller than nx");
     if ((long long)ny * pitch >= (1LL << 31)) return fail(PXB_ERR_ARG, "planes of 2^31 elements or more are not supported");
@@ -381,15 +461,29 @@ int common_setup(PlanCommon& P, int ny, int nx, long long pitch, int dtype, doub
     int dev = 0;
     PXB_CUDA(cudaGetDevice(&dev));
     PXB_CUDA(cudaDeviceGetAttribute(&P.sm_count, cudaDevAttrMultiProcessorCount, dev));
+    if (want_path < PXB_PATH_AUTO || want_path > PXB_PATH_GENERAL || (roe && want_path == PXB_PATH_GENERAL))
+        return fail(PXB_ERR_ARG, "unknown stage path");
+    for (int k = 0; k < nh; ++k)
+        if (!kind_ok(hs[k].kind, roe))
+            return fail(PXB_ERR_ARG, "boundary handler " + std::to_string(k) + " has kind " + std::to_string(hs[k].kind) +
+                                         (roe ? ", not a \"Roe\" handler" : ", not a \"Roe Exner\" handler"));
+    path = want_path == PXB_PATH_GENERAL ? PXB_PATH_GENERAL : PXB_PATH_FUSED;
     if (nh > 0) {
-        Resolved R = resolve(hs, nh, ny, nx, pitch, roe, !roe);
-        if (!R.error.empty()) return fail(PXB_ERR_UNSUPPORTED, R.error);
         int maxcount = 0;
         int st = upload_handlers(hs, nh, (long long)(ny - 1) * pitch + nx, P.handlers, maxcount);
         if (st != PXB_OK) return st;
-        PXB_CUDA(cudaMalloc(&P.ring, sizeof(pxb_ring_recipe) * R.ring.size()));
-        PXB_CUDA(cudaMemcpy(P.ring, R.ring.data(), sizeof(pxb_ring_recipe) * R.ring.size(), cudaMemcpyHostToDevice));
         PXB_CUDA(cudaMalloc(&P.bc_tmp, 6 * (size_t)std::max(1, maxcount) * P.esize()));
+        if (path == PXB_PATH_FUSED) {
+            Resolved R = resolve(hs, nh, ny, nx, pitch, roe, !roe);
+            if (!R.error.empty()) {
+                if (want_path == PXB_PATH_FUSED || roe) return fail(PXB_ERR_UNSUPPORTED, R.error);
+                path = PXB_PATH_GENERAL;
+            } else {
+                PXB_CUDA(cudaMalloc(&P.ring, sizeof(pxb_ring_recipe) * R.ring.size()));
+                PXB_CUDA(cudaMemcpy(P.ring, R.ring.data(), sizeof(pxb_ring_recipe) * R.ring.size(),
+                                    cudaMemcpyHostToDevice));
+            }
+        }
     }
     PXB_CUDA(cudaMalloc(&P.scr, sizeof(pxb::CflScratch)));
     PXB_CUDA(cudaMemset(P.scr, 0, sizeof(pxb::CflScratch)));
@@ -450,6 +544,8 @@ int set_error(int code, const std::string& msg) { return fail(code, msg); }
 // =====================================================================================
 struct pxb_re_plan {
     PlanCommon c;
+    int path = PXB_PATH_FUSED;
+    void* gen = nullptr;  // general path: 7 scratch planes (h, hu, hv, z_b, G, n, z_b after Exner)
     int mpm = 0;
     const uint8_t* nodata = nullptr;
     Geometry stage[8];  // by (mpm, mask, avg) variant: band geometry from its occupancy
@@ -543,6 +639,95 @@ int re_stage_impl(pxb_re_plan* P, const pxb_re_fields* in, const pxb_re_fields* 
     return PXB_OK;
 }
 
+// Every handler in order on the field slots f (h, hu, hv, z_b, n, G), at the time *tptr
+// (device) or tval.
+template <class T>
+int apply_handlers(PlanCommon& C, T* const f[6], const double* tptr, double tval, cudaStream_t s) {
+    for (auto& h : C.handlers) {
+        pxb::BcArgs<T> b{};
+        for (int k = 0; k < 6; ++k) b.f[k] = f[k];
+        b.cells = h.cells;
+        b.donors = h.donors;
+        b.count = h.count;
+        b.kind = h.kind;
+        b.nx = (T)h.nx;
+        b.ny = (T)h.ny;
+        b.c0 = (T)h.c0;
+        b.c1 = (T)h.c1;
+        b.q = (T)h.q;
+        b.vx = (T)h.vx;
+        b.vy = (T)h.vy;
+        b.neg_alpha = h.neg_alpha;
+        b.zb0 = h.zb0;
+        b.hb = (T)h.hb;
+        b.tptr = tptr;
+        b.tval = tval;
+        b.tmp = (T*)C.bc_tmp;
+        PXB_CUDA(pxb::launch_bc<T>(b, s));
+    }
+    return PXB_OK;
+}
+
+// One stage on the general path (re_general.cuh).
+template <class T>
+int re_general_impl(pxb_re_plan* P, const pxb_re_fields* in, const pxb_re_fields* out, const pxb_re_fields* avg,
+                    const void* dt, const double* tptr, double tval, cudaStream_t s) {
+    const size_t plane = (size_t)P->c.ny * (size_t)P->c.pitch;
+    T* S = (T*)P->gen;
+    pxb::GenArgs<T> a{};
+    a.ny = P->c.ny;
+    a.nx = P->c.nx;
+    a.pitch = P->c.pitch;
+    a.dx = (T)P->c.dx;
+    a.h = (const T*)in->h;
+    a.hu = (const T*)in->hu;
+    a.hv = (const T*)in->hv;
+    a.zb = (const T*)in->z_b;
+    a.z = (const T*)in->z;
+    a.nb = (const T*)in->n_b;
+    a.G = (const T*)in->G;
+    a.n = (const T*)in->n;
+    a.sh = S;
+    a.shu = S + plane;
+    a.shv = S + 2 * plane;
+    a.szb = S + 3 * plane;
+    a.sG = S + 4 * plane;
+    a.sn = S + 5 * plane;
+    a.szb2 = S + 6 * plane;
+    a.nodata = P->nodata;
+    a.dt = (const T*)dt;
+    a.sed = sed_of<T>(P);
+    a.mpm = P->mpm;
+    a.oh = (T*)out->h;
+    a.ohu = (T*)out->hu;
+    a.ohv = (T*)out->hv;
+    a.ozb = (T*)out->z_b;
+    a.oG = (T*)out->G;
+    // n is carried when the input has it (and the partner too, for an averaged stage)
+    a.on = (in->n && (!avg || avg->n)) ? (T*)out->n : nullptr;
+    if (avg) {
+        a.ah = (const T*)avg->h;
+        a.ahu = (const T*)avg->hu;
+        a.ahv = (const T*)avg->hv;
+        a.azb = (const T*)avg->z_b;
+        a.aG = (const T*)avg->G;
+        a.an = (const T*)avg->n;
+    }
+    a.err = &P->c.scr->err;
+    PXB_CUDA(pxb::launch_re_general<T>(a, pxb::GEN_HYDRO, s));
+    PXB_CUDA(pxb::launch_re_general<T>(a, pxb::GEN_CORR, s));
+    T* const f1[6] = {a.sh, a.shu, a.shv, a.szb, a.sn, a.sG};
+    int st = apply_handlers<T>(P->c, f1, tptr, tval, s);
+    if (st != PXB_OK) return st;
+    PXB_CUDA(pxb::launch_re_general<T>(a, pxb::GEN_GRASS, s));
+    PXB_CUDA(pxb::launch_re_general<T>(a, pxb::GEN_EXNER, s));
+    T* const f2[6] = {a.sh, a.shu, a.shv, a.szb2, a.sn, a.sG};
+    st = apply_handlers<T>(P->c, f2, tptr, tval, s);
+    if (st != PXB_OK) return st;
+    PXB_CUDA(pxb::launch_re_general<T>(a, pxb::GEN_STORE, s));
+    return PXB_OK;
+}
+
 template <class T>
 int re_init_impl(pxb_re_plan* P, const pxb_re_fields* f, cudaStream_t s) {
     pxb::InitArgs<T> a{};
@@ -560,50 +745,50 @@ int re_init_impl(pxb_re_plan* P, const pxb_re_fields* f, cudaStream_t s) {
     a.mpm = P->mpm;
     a.sed = sed_of<T>(P);
     PXB_CUDA(pxb::launch_re_init<T>(a, s));
-    for (auto& h : P->c.handlers) {
-        pxb::BcArgs<T> b{};
-        b.f[0] = (T*)f->h;
-        b.f[1] = (T*)f->hu;
-        b.f[2] = (T*)f->hv;
-        b.f[3] = (T*)f->z_b;
-        b.f[4] = (T*)f->n;
-        b.f[5] = (T*)f->G;
-        b.cells = h.cells;
-        b.donors = h.donors;
-        b.count = h.count;
-        b.kind = h.kind;
-        b.nx = (T)h.nx;
-        b.ny = (T)h.ny;
-        b.c0 = (T)h.c0;
-        b.c1 = (T)h.c1;
-        b.tmp = (T*)P->c.bc_tmp;
-        PXB_CUDA(pxb::launch_bc<T>(b, s));
-    }
-    return PXB_OK;
+    T* const fs[6] = {(T*)f->h, (T*)f->hu, (T*)f->hv, (T*)f->z_b, (T*)f->n, (T*)f->G};
+    return apply_handlers<T>(P->c, fs, nullptr, 0.0, s);
+}
+
+// One stage on the plan's path; the general path reads the time from *tptr or tval.
+int re_stage_any(pxb_re_plan* P, const pxb_re_fields* in, const pxb_re_fields* out, const pxb_re_fields* avg,
+                 const void* dt, const double* tptr, double tval, cudaStream_t s) {
+    const bool f64 = P->c.dtype == PXB_F64;
+    if (P->path == PXB_PATH_GENERAL)
+        return f64 ? re_general_impl<double>(P, in, out, avg, dt, tptr, tval, s)
+                   : re_general_impl<float>(P, in, out, avg, dt, tptr, tval, s);
+    return f64 ? re_stage_impl<double>(P, in, out, avg, dt, s) : re_stage_impl<float>(P, in, out, avg, dt, s);
 }
 
 int re_steps(pxb_re_plan* P, const pxb_re_fields* A, const pxb_re_fields* B, int nsteps, int scheme, double cfl,
-             void* dt_log, cudaStream_t s) {
+             double t0, void* dt_log, cudaStream_t s) {
     const bool f64 = P->c.dtype == PXB_F64;
+    const bool general = P->path == PXB_PATH_GENERAL;
     auto cfl_call = [&](const pxb_re_fields* f, cudaStream_t st) {
         return f64 ? re_cfl_impl<double>(P, f, cfl, P->c.dt_dev, dt_log, st)
                    : re_cfl_impl<float>(P, f, cfl, P->c.dt_dev, dt_log, st);
     };
+    // the time of the step is the one the CFL launch before the stage recorded
+    const double* tdev = &P->c.scr->t_step;
     auto stage_call = [&](const pxb_re_fields* in, const pxb_re_fields* out, const pxb_re_fields* avg,
-                          cudaStream_t st) {
-        return f64 ? re_stage_impl<double>(P, in, out, avg, P->c.dt_dev, st)
-                   : re_stage_impl<float>(P, in, out, avg, P->c.dt_dev, st);
-    };
-    // static planes of b are those of a
+                          cudaStream_t st) { return re_stage_any(P, in, out, avg, P->c.dt_dev, tdev, 0.0, st); };
+    // static planes of b are those of a; the general path carries n in b as well
     pxb_re_fields Bs = *B;
     Bs.z = A->z;
     Bs.n_b = A->n_b;
-    Bs.n = A->n;
+    if (general) {
+        if (A->n && (!B->n || B->n == A->n))
+            return fail(PXB_ERR_ARG, "the general stage path needs b->n distinct from a->n");
+    } else {
+        Bs.n = A->n;
+    }
     const double cfl_d = cfl;
-    std::vector<const void*> key = {A->h, A->hu, A->hv, A->z_b, A->G, A->z, A->n_b, B->h, B->hu, B->hv, B->z_b,
-                                    B->G, dt_log, (const void*)(intptr_t)scheme};
+    std::vector<const void*> key = {A->h, A->hu, A->hv, A->z_b, A->G, A->z, A->n_b, A->n, B->h, B->hu, B->hv,
+                                    B->z_b, B->G, Bs.n, dt_log, (const void*)(intptr_t)scheme};
     key.push_back(*(const void* const*)&cfl_d);
     PXB_CUDA(cudaMemsetAsync(&P->c.scr->step, 0, sizeof(unsigned int), s));
+    // only the general path has handlers that read the time
+    if (general)
+        PXB_CUDA(f64 ? pxb::launch_set_time<double>(P->c.scr, t0, s) : pxb::launch_set_time<float>(P->c.scr, t0, s));
     if (scheme == PXB_SSPRK2) {
         pxb_re_fields B1 = Bs;
         if (P->mpm) B1.G = nullptr;  // stage-1 G is recomputed by stage 2
@@ -627,9 +812,10 @@ int re_steps(pxb_re_plan* P, const pxb_re_fields* A, const pxb_re_fields* B, int
     if (r == PXB_OK) r = stage_call(A, &Bs, nullptr, s);
     if (r != PXB_OK) return r;
     const size_t es = P->c.esize();
-    const void* src[5] = {Bs.h, Bs.hu, Bs.hv, Bs.z_b, Bs.G};
-    void* dst[5] = {A->h, A->hu, A->hv, A->z_b, A->G};
-    for (int k = 0; k < 5; ++k)
+    const void* src[6] = {Bs.h, Bs.hu, Bs.hv, Bs.z_b, Bs.G, Bs.n};
+    void* dst[6] = {A->h, A->hu, A->hv, A->z_b, A->G, A->n};
+    const int ncopy = (general && A->n) ? 6 : 5;
+    for (int k = 0; k < ncopy; ++k)
         PXB_CUDA(cudaMemcpy2DAsync(dst[k], P->c.pitch * es, src[k], P->c.pitch * es, P->c.nx * es, P->c.ny,
                                    cudaMemcpyDeviceToDevice, s));
     return PXB_OK;
@@ -708,8 +894,14 @@ int pxb_re_plan_create(const pxb_re_config* cfg, pxb_re_plan** out) {
     if (cfg->mpm && (!cfg->seds || cfg->nsed < 1 || cfg->nsed > PXB_MAX_SED))
         return fail(PXB_ERR_ARG, "MPM needs 1..8 sediment classes");
     pxb_re_plan* P = new pxb_re_plan();
-    int st = common_setup(P->c, cfg->ny, cfg->nx, cfg->pitch, cfg->dtype, cfg->dx, cfg->handlers, cfg->nhandlers, false);
+    int st = common_setup(P->c, cfg->ny, cfg->nx, cfg->pitch, cfg->dtype, cfg->dx, cfg->handlers, cfg->nhandlers, false,
+                          cfg->stage_path, P->path);
+    if (st == PXB_OK && P->path == PXB_PATH_GENERAL) {
+        const cudaError_t e = cudaMalloc(&P->gen, 7 * (size_t)cfg->ny * (size_t)cfg->pitch * P->c.esize());
+        if (e != cudaSuccess) st = fail(PXB_ERR_CUDA, std::string("scratch planes: ") + cudaGetErrorString(e));
+    }
     if (st != PXB_OK) {
+        cudaFree(P->gen);
         P->c.release();
         delete P;
         return st;
@@ -739,9 +931,12 @@ int pxb_re_plan_destroy(pxb_re_plan* plan) {
     if (!plan) return PXB_OK;
     cudaDeviceSynchronize();
     plan->c.release();
+    cudaFree(plan->gen);
     delete plan;
     return PXB_OK;
 }
+
+int pxb_re_plan_path(const pxb_re_plan* plan) { return plan ? plan->path : 0; }
 
 int pxb_re_init(pxb_re_plan* P, const pxb_re_fields* f, void* stream) {
     if (!P) return fail(PXB_ERR_ARG, "null plan");
@@ -763,7 +958,7 @@ int pxb_re_cfl(pxb_re_plan* P, const pxb_re_fields* f, double cfl, void* dt_dev,
 }
 
 int pxb_re_stage(pxb_re_plan* P, const pxb_re_fields* in, const pxb_re_fields* out, const pxb_re_fields* avg,
-                 const void* dt_dev, void* stream) {
+                 const void* dt_dev, double time, void* stream) {
     if (!P) return fail(PXB_ERR_ARG, "null plan");
     int st = check_fields(in, !P->mpm);
     if (st) return st;
@@ -774,13 +969,13 @@ int pxb_re_stage(pxb_re_plan* P, const pxb_re_fields* in, const pxb_re_fields* o
     if (!dt_dev) return fail(PXB_ERR_ARG, "dt_dev is null");
     if (in->h == out->h || in->hu == out->hu || in->hv == out->hv || in->z_b == out->z_b)
         return fail(PXB_ERR_ARG, "stage output must not alias its input");
-    cudaStream_t s = (cudaStream_t)stream;
-    return P->c.dtype == PXB_F64 ? re_stage_impl<double>(P, in, out, avg, dt_dev, s)
-                                 : re_stage_impl<float>(P, in, out, avg, dt_dev, s);
+    if (P->path == PXB_PATH_GENERAL && in->n && out->n == in->n)
+        return fail(PXB_ERR_ARG, "stage output n must not alias its input on the general path");
+    return re_stage_any(P, in, out, avg, dt_dev, nullptr, time, (cudaStream_t)stream);
 }
 
 int pxb_re_run(pxb_re_plan* P, const pxb_re_fields* a, const pxb_re_fields* b, int32_t nsteps, int32_t scheme,
-               double cfl, void* dt_log, void* stream) {
+               double cfl, double t0, void* dt_log, void* stream) {
     if (!P) return fail(PXB_ERR_ARG, "null plan");
     int st = check_fields(a, true);
     if (st) return st;
@@ -790,7 +985,7 @@ int pxb_re_run(pxb_re_plan* P, const pxb_re_fields* a, const pxb_re_fields* b, i
     if (nsteps < 0) return fail(PXB_ERR_ARG, "nsteps < 0");
     if (scheme != PXB_FE && scheme != PXB_SSPRK2) return fail(PXB_ERR_ARG, "scheme must be PXB_FE or PXB_SSPRK2");
     if (nsteps == 0) return PXB_OK;
-    return re_steps(P, a, b, nsteps, scheme, cfl, dt_log, (cudaStream_t)stream);
+    return re_steps(P, a, b, nsteps, scheme, cfl, t0, dt_log, (cudaStream_t)stream);
 }
 
 int pxb_re_check(pxb_re_plan* P, void* stream) {
@@ -802,7 +997,9 @@ int pxb_roe_plan_create(const pxb_roe_config* cfg, pxb_roe_plan** out) {
     if (!cfg || !out) return fail(PXB_ERR_ARG, "null config or output pointer");
     *out = nullptr;
     pxb_roe_plan* P = new pxb_roe_plan();
-    int st = common_setup(P->c, cfg->ny, cfg->nx, cfg->pitch, cfg->dtype, cfg->dx, cfg->handlers, cfg->nhandlers, true);
+    int path = 0;
+    int st = common_setup(P->c, cfg->ny, cfg->nx, cfg->pitch, cfg->dtype, cfg->dx, cfg->handlers, cfg->nhandlers, true,
+                          PXB_PATH_FUSED, path);
     if (st != PXB_OK) {
         P->c.release();
         delete P;

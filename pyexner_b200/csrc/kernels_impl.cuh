@@ -79,6 +79,25 @@ cudaError_t launch_bc(const BcArgs<T>& a, cudaStream_t s) {
 }
 
 template <class T>
+cudaError_t launch_re_general(const GenArgs<T>& a, int phase, cudaStream_t s) {
+    dim3 b(32, 8), g((a.nx + 31) / 32, (a.ny + 7) / 8);
+    switch (phase) {
+        case GEN_HYDRO: gen_hydro_kernel<T><<<g, b, 0, s>>>(a); break;
+        case GEN_CORR: gen_corr_kernel<T><<<g, b, 0, s>>>(a); break;
+        case GEN_GRASS: gen_grass_kernel<T><<<g, b, 0, s>>>(a); break;
+        case GEN_EXNER: gen_exner_kernel<T><<<g, b, 0, s>>>(a); break;
+        default: gen_store_kernel<T><<<g, b, 0, s>>>(a); break;
+    }
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t launch_set_time(CflScratch* scr, double t0, cudaStream_t s) {
+    set_time_kernel<T><<<1, 1, 0, s>>>(scr, t0);
+    return cudaGetLastError();
+}
+
+template <class T>
 cudaError_t launch_roe_stage(const RoeArgs<T>& a, bool avg, cudaStream_t s) {
     dim3 b(32, 8), g((a.nx + 31) / 32, (a.ny + 7) / 8);
     if (avg) roe_stage_kernel<T, true><<<g, b, 0, s>>>(a);
@@ -99,6 +118,8 @@ cudaError_t launch_roe_cfl(const CflArgs<T>& a, int grid, cudaStream_t s) {
     template int re_cfl_blocks_per_sm<T>(bool);                                                         \
     template cudaError_t launch_re_init<T>(const InitArgs<T>&, cudaStream_t);                           \
     template cudaError_t launch_bc<T>(const BcArgs<T>&, cudaStream_t);                                  \
+    template cudaError_t launch_re_general<T>(const GenArgs<T>&, int, cudaStream_t);                    \
+    template cudaError_t launch_set_time<T>(CflScratch*, double, cudaStream_t);                         \
     template cudaError_t launch_roe_stage<T>(const RoeArgs<T>&, bool, cudaStream_t);                    \
     template cudaError_t launch_roe_cfl<T>(const CflArgs<T>&, int, cudaStream_t);
 

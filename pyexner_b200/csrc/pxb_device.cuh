@@ -452,7 +452,7 @@ __device__ __forceinline__ void cubic_extremes(T ut, T at, T ct, T& lmin, T& lma
     const T c = (T(1) + at) * (ct * ct) - ut * ut;
     const T d = -(ct * ct) * at * ut;
     const T p = (T(-3) * c - b * b) / T(3);
-    const T q = (T(2) * d_pow(b, T(3)) - T(-9) * b * c + T(27) * d) / T(-27);
+    const T q = (T(2) * (b * (b * b)) - T(-9) * b * c + T(27) * d) / T(-27);
     const T x = clip1((T(3) * q) / (T(2) * p) * d_sqrt(T(-3) / p));
     const T th = d_acos(x);
     const T sq = T(2) * d_sqrt(-p / T(3));

@@ -4,6 +4,7 @@
 
 #include "init_bc.cuh"
 #include "re_cfl.cuh"
+#include "re_general.cuh"
 #include "re_stage.cuh"
 #include "roe_plain.cuh"
 
@@ -26,6 +27,12 @@ template <class T>
 cudaError_t launch_re_init(const InitArgs<T>& a, cudaStream_t s);
 template <class T>
 cudaError_t launch_bc(const BcArgs<T>& a, cudaStream_t s);
+// Phases of the general stage path (re_general.cuh).
+enum GenPhase { GEN_HYDRO = 0, GEN_CORR = 1, GEN_GRASS = 2, GEN_EXNER = 3, GEN_STORE = 4 };
+template <class T>
+cudaError_t launch_re_general(const GenArgs<T>& a, int phase, cudaStream_t s);
+template <class T>
+cudaError_t launch_set_time(CflScratch* scr, double t0, cudaStream_t s);
 template <class T>
 cudaError_t launch_roe_stage(const RoeArgs<T>& a, bool avg, cudaStream_t s);
 template <class T>

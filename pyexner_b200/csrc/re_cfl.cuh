@@ -22,7 +22,16 @@ struct CflScratch {
     unsigned int step;           // index into the dt log
     int err;                     // sticky error word
     int pad;
+    double t_step;               // simulation time at the start of the current step
+    double t_next;               // t_step + dt: the time the next dt is added to
 };
+
+// Start of a fixed-step run at time t0 (the first CFL launch moves it into t_step).
+template <class T>
+__global__ void set_time_kernel(CflScratch* scr, double t0) {
+    scr->t_step = t0;
+    scr->t_next = t0;
+}
 
 template <class T>
 struct CflArgs {
@@ -121,6 +130,9 @@ __global__ void __launch_bounds__(256) re_cfl_kernel(const CflArgs<T> a) {
         *a.dt_out = dt;
         if (a.dt_log) a.dt_log[a.scr->step] = dt;
         a.scr->step += 1;
+        // time of this step, accumulated in float64 like the host loops of the integrators
+        a.scr->t_step = a.scr->t_next;
+        a.scr->t_next = a.scr->t_next + (double)dt;
         if (!d_isfinite(dt)) a.scr->err |= 2;
         a.scr->maxbits = 0ull;
         a.scr->done = 0u;

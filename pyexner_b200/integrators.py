@@ -74,8 +74,9 @@ def scratch_like(state):
     return type(state)(**kw)
 
 
-def run_steps(state, mask, solver_config, scheme, n_steps, cfl, scratch=None, log_dt=True):
-    """Advance ``state`` IN PLACE by ``n_steps`` steps on the device.
+def run_steps(state, mask, solver_config, scheme, n_steps, cfl, scratch=None, log_dt=True, t0=0.0):
+    """Advance ``state`` IN PLACE by ``n_steps`` steps on the device, starting at time
+    ``t0`` (the step times are accumulated on the device).
 
     Returns the device tensor of the dts taken (or None).  ``scratch`` is a second
     state of the same layout (allocated when not given)."""
@@ -86,7 +87,7 @@ def run_steps(state, mask, solver_config, scheme, n_steps, cfl, scratch=None, lo
     if isinstance(state, RoeExnerState):
         plan = _re_plan(state, mask, solver_config)
         _lib.call("pxb_re_run", plan.handle, ctypes.byref(state.c_fields()), ctypes.byref(b.c_fields()),
-                  int(n_steps), code, float(cfl), dptr, _stream())
+                  int(n_steps), code, float(cfl), float(t0), dptr, _stream())
     else:
         plan = _roe_plan(state, solver_config)
         _lib.call("pxb_roe_run", plan.handle, ctypes.byref(state.c_fields()), ctypes.byref(b.c_fields()),

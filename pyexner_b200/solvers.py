@@ -11,8 +11,10 @@ the one PyExner's Forward Euler integrator drives (forwardeuler.py:39-40, 59, 97
     step_fn(state, time, dt, mask, config) -> state
     compute_dt_fn(state, cfl, mask, config) -> 0-d device tensor
 
-Every compute call goes through the C ABI; there is no host fallback.  ``time`` is
-accepted for signature parity: none of the handlers on this path depends on it.
+Every compute call goes through the C ABI; there is no host fallback.  ``time`` reaches
+the time-dependent handlers (Berthon, NormalFlowDepth).  A plan runs the fused stage
+kernel when its boundary layout allows it and the general kernel chain otherwise
+(``stage_path`` "auto"); "fused" or "general" force one.
 """
 from __future__ import annotations
 
@@ -36,6 +38,7 @@ class SolverConfig(NamedTuple):
     compute_n: object = None
     plans: dict = None        # plan cache of the config (per dtype / mask)
     band_rows: int = 0        # rows per warp band of the stage kernel (0 = sized to the device)
+    stage_path: int = 0       # _lib.PATH_AUTO / PATH_FUSED / PATH_GENERAL
 
 
 class SolverBundle(NamedTuple):
@@ -85,7 +88,7 @@ def _dtype_code(t):
 class RePlan:
     """Owner of one ``pxb_re_plan`` (boundary recipes, CFL scratch, graphs)."""
 
-    def __init__(self, state, mask, config, band_rows=0):
+    def __init__(self, state, mask, config, band_rows=0, stage_path=0):
         ny, nx = state.shape
         self.mpm = isinstance(config.compute_G, str)
         nod = None
@@ -110,9 +113,11 @@ class RePlan:
         cfg.handlers = handlers if nh else None
         cfg.nhandlers = nh
         cfg.band_rows = int(band_rows)
+        cfg.stage_path = int(stage_path)
         h = ctypes.c_void_p()
         _lib.call("pxb_re_plan_create", ctypes.byref(cfg), ctypes.byref(h))
         self.handle = h
+        self.path = _lib.load().pxb_re_plan_path(h)
         self.dtype = state.dtype
         self.device = state.h.device
 
@@ -131,10 +136,22 @@ def _re_plan(state, mask, config):
     key = (state.dtype, state.shape, state.pitch, None if mask is None else mask.data_ptr())
     plans = config.plans
     if plans is None:
-        return RePlan(state, mask, config, config.band_rows)
+        return RePlan(state, mask, config, config.band_rows, config.stage_path)
     if key not in plans:
-        plans[key] = RePlan(state, mask, config, config.band_rows)
+        plans[key] = RePlan(state, mask, config, config.band_rows, config.stage_path)
     return plans[key]
+
+
+_PATHS = {"auto": _lib.PATH_AUTO, "fused": _lib.PATH_FUSED, "general": _lib.PATH_GENERAL}
+
+
+def stage_path_code(v):
+    """``stage_path`` parameter ("auto" / "fused" / "general" or the integer code)."""
+    if isinstance(v, str):
+        if v.lower() not in _PATHS:
+            raise ValueError(f"unknown stage_path '{v}'. Available options: {list(_PATHS)}")
+        return _PATHS[v.lower()]
+    return int(v)
 
 
 def get_mask(state, mpi_handler=None, b_mask=None):
@@ -147,7 +164,8 @@ def get_mask(state, mpi_handler=None, b_mask=None):
 def config_fn_roeexner(state, mpi_handler, boundaries, dx, params):
     grass = params.get("erosion", {}).get("grass_factor", 0.0)
     return SolverConfig(mpi_handler=mpi_handler, boundaries=boundaries, dx=float(dx), halo_exchange=_identity,
-                        compute_G=grass, compute_n=grass, plans={}, band_rows=int(params.get("band_rows", 0)))
+                        compute_G=grass, compute_n=grass, plans={}, band_rows=int(params.get("band_rows", 0)),
+                        stage_path=stage_path_code(params.get("stage_path", "auto")))
 
 
 def init_fn_roeexner(state, mask, config):
@@ -170,11 +188,14 @@ def step_fn_roeexner(state, time, dt, mask, config, avg=None):
     0.5*avg + 0.5*stage(state) is returned instead."""
     plan = _re_plan(state, mask, config)
     ny, nx = state.shape
-    new = {f: alloc_plane(ny, nx, state.dtype, state.h.device) for f in ("h", "hu", "hv", "z_b", "G")}
+    # the general path carries n through the handlers; the fused path leaves it as it is
+    fields = ("h", "hu", "hv", "z_b", "G") + (("n",) if plan.path == _lib.PATH_GENERAL else ())
+    new = {f: alloc_plane(ny, nx, state.dtype, state.h.device) for f in fields}
     out = state.replace(**new)
     dtt = _dt_tensor(dt, state)
     _lib.call("pxb_re_stage", plan.handle, ctypes.byref(state.c_fields()), ctypes.byref(out.c_fields()),
-              ctypes.byref(avg.c_fields()) if avg is not None else None, ctypes.c_void_p(dtt.data_ptr()), _stream())
+              ctypes.byref(avg.c_fields()) if avg is not None else None, ctypes.c_void_p(dtt.data_ptr()),
+              float(time), _stream())
     return out
 
 

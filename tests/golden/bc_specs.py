@@ -107,7 +107,56 @@ def refl_self(ny, nx):
     }
 
 
+def berthon_like(ny, nx):
+    """The inlet / outlet layout of the reference's Berthon analytic case
+    (tests/runtime/2D_const_flux/input.yaml): ConstantInflux + Berthon bed on the left,
+    NormalFlowDepth on the right, reflective walls."""
+    return {
+        "inlet_flux": _b("ConstantInflux", left(ny, nx), [-1.0, 0.0], values=(1.0, 1.0, 0.0)),
+        "inlet_bed": _b("Berthon", left(ny, nx), [-1.0, 0.0], values=(1.0, 0.005, 0.005, 0.005, 1, 0.0)),
+        "outlet_bed": _b("NormalFlowDepth", right(ny, nx), [1.0, 0.0],
+                         values=(1.0, 0.005, 0.005, 0.005, 1, float(nx - 1))),
+        "bottom": _b("Reflective", bottom(ny, nx), [0.0, -1.0]),
+        "top": _b("Reflective", top(ny, nx), [0.0, 1.0]),
+    }
+
+
+def outflux_steep(ny, nx):
+    """ConstantOutflux + SteepFall outlet, zero-momentum walls (one with NaN values,
+    which leaves the momentum as it is)."""
+    return {
+        "inlet": _b("ConstantInflux", left(ny, nx), [-1.0, 0.0], values=(0.3, 1.0, 0.0)),
+        "inlet_bed": _b("TransmissiveBed", left(ny, nx), [-1.0, 0.0]),
+        "outlet": _b("ConstantOutflux", right(ny, nx), [1.0, 0.0], values=(0.3, 1.0, 0.0)),
+        "fall": _b("SteepFall", right(ny, nx), [1.0, 0.0]),
+        "top": _b("ZeroMomentum", top(ny, nx), [0.0, 1.0], values=(0.0, 0.0, 0.0, 0.0)),
+        "bottom_keep": _b("ZeroMomentum", bottom(ny, nx), [0.0, -1.0],
+                          values=("nan", "nan", "nan", "nan")),
+        "bottom": _b("Reflective", bottom(ny, nx), [0.0, -1.0]),
+    }
+
+
+def l_domain(ny, nx):
+    """An L-shaped domain: the top-right block (rows 0-5, columns >= nx-6) has a NaN bed
+    (nodata); walls follow the L, including an interior wall along the block's left side
+    and an interior floor under it, as in the reference's L-domain cases."""
+    bx0 = nx - 6  # first nodata column
+    return {
+        "left": _b("Reflective", left(ny, nx), [-1.0, 0.0]),
+        "bottom": _b("Reflective", bottom(ny, nx), [0.0, -1.0]),
+        "top": _b("Reflective", top(ny, nx, cols=(0, bx0 - 1)), [0.0, 1.0]),
+        "right": _b("Reflective", right(ny, nx, rows=(6, ny - 1)), [1.0, 0.0]),
+        "internal_wall": _b("Reflective", [[bx0 - 1.5, ny - 6.5], [bx0 - 0.5, ny - 6.5], [bx0 - 0.5, ny - 1.5],
+                                            [bx0 - 1.5, ny - 1.5]], [1.0, 0.0]),
+        "internal_floor": _b("Reflective", [[bx0 - 0.5, ny - 7.5], [nx - 1.5, ny - 7.5], [nx - 1.5, ny - 6.5],
+                                             [bx0 - 0.5, ny - 6.5]], [0.0, 1.0]),
+    }
+
+
 BC_SPECS = {
+    "berthon_like": berthon_like,
+    "outflux_steep": outflux_steep,
+    "l_domain": l_domain,
     "refl_self": refl_self,
     "trans_x_refl_y": trans_x_refl_y,
     "refl_first": refl_first,

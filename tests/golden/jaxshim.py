@@ -11,6 +11,8 @@ It is used only by ``tests/golden/make_golden.py`` to generate the golden vector
 that pin the oracle.  Nothing in the product imports it.
 
 Semantics kept from JAX:
+  * ``x ** k`` with a Python int ``k`` is ``lax.integer_pow`` (repeated multiplication);
+    other exponents go to ``pow``.
   * ``x.at[idx].set(v)`` / ``.add(v)`` are functional (return a new array);
     ``.add`` accumulates duplicates like ``jax.numpy`` scatter-add.
   * ``jit`` / ``vmap`` / ``lax.fori_loop`` / ``lax.while_loop`` have their
@@ -32,6 +34,29 @@ class JArr(np.ndarray):
     @property
     def at(self):
         return _At(self)
+
+    def __pow__(self, y):
+        # ``x ** k`` with a Python int k is ``lax.integer_pow`` in JAX: powering by
+        # repeated multiplication, not a call of pow().
+        if isinstance(y, int) and not isinstance(y, bool):
+            return _integer_pow(self, y)
+        return _wrap(np.power(self, y))
+
+
+def _integer_pow(x, y):
+    """jax.lax.integer_pow: binary powering (x**3 = x * (x * x)), reciprocal for y < 0."""
+    if y == 0:
+        return _wrap(np.ones_like(x))
+    recip = y < 0
+    y = -y if recip else y
+    acc = None
+    while y > 0:
+        if y & 1:
+            acc = x if acc is None else np.multiply(acc, x)
+        y >>= 1
+        if y > 0:
+            x = np.multiply(x, x)
+    return _wrap(np.divide(np.ones_like(acc), acc) if recip else acc)
 
 
 class _At:
@@ -68,6 +93,8 @@ class _AtIdx:
 def _wrap(x):
     if isinstance(x, np.ndarray) and not isinstance(x, JArr):
         return x.view(JArr)
+    if isinstance(x, np.floating):  # jax returns 0-d arrays, not numpy scalars
+        return np.asarray(x).view(JArr)
     if isinstance(x, tuple):
         return tuple(_wrap(i) for i in x)
     if isinstance(x, list):

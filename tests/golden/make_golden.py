@@ -103,6 +103,12 @@ def make_state_arrays(rng, ny, nx, regime):
     return dict(h=h, hu=hu, hv=hv, z=z, z_b=zb, n=n)
 
 
+def l_block(arrs):
+    """NaN bed in the top-right 6 x 6 block (the outside of an L-shaped domain)."""
+    arrs["z"][:6, -6:] = np.nan
+    return arrs
+
+
 SEDS_MPM = {
     "one": {"s1": dict(fraction=1.0, diameter=1.61e-3, density=2630.0, deposition_flux=0.0, erosion_flux=0.0)},
     "two": {
@@ -142,6 +148,9 @@ CASES = [
     ("const_wetdry_nodata", (12, 12), "wetdry", "partial_nodata", dict(grass_factor=0.01)),
     ("mpm1_fast_reflfirst", (11, 12), "fast", "refl_first", dict(grass_factor="MPM", bulk_porosity=0.42, sediments=SEDS_MPM["one"])),
     ("const_fast_selfrefl", (12, 14), "fast", "refl_self", dict(grass_factor=0.005)),
+    ("const_smooth_berthon", (10, 16), "smooth", "berthon_like", dict(grass_factor=0.005)),
+    ("mpm1_fast_outflux", (12, 15), "fast", "outflux_steep", dict(grass_factor="MPM", bulk_porosity=0.42, sediments=SEDS_MPM["one"])),
+    ("mpm1_fast_ldomain", (14, 16), "fast", "l_domain", dict(grass_factor="MPM", bulk_porosity=0.42, sediments=SEDS_MPM["one"])),
 ]
 
 DX = 0.1
@@ -178,6 +187,8 @@ def run_roe_exner_cases(mods):
     for ci, (name, (ny, nx), regime, bcname, erosion) in enumerate(CASES):
         rng = np.random.default_rng(1000 + ci)
         arrs = make_state_arrays(rng, ny, nx, regime)
+        if bcname == "l_domain":
+            arrs = l_block(arrs)
         X, Y = grid_coords(ny, nx)
         params = dict(flux_scheme="Roe Exner", boundaries=BC_SPECS[bcname](ny, nx), erosion=erosion)
         bm = mods.b.BoundaryManager(params, J(X), J(Y))
@@ -203,24 +214,28 @@ def run_roe_exner_cases(mods):
             out[f"corr_{f}"] = np.asarray(getattr(st_c, f))
         st1 = s.step_fn_roeexner(st, 0.0, dt, mask, cfg)
         dump_state("stage1", st1, out)
-        # Forward Euler, fixed step count
+        # Forward Euler, fixed step count; the time argument is the time at the step start
         fe = st
         dts = []
+        t = 0.0
         for _ in range(NSTEPS):
             d = s.compute_dt_roeexner(fe, CFL, mask, cfg)
-            fe = s.step_fn_roeexner(fe, 0.0, d, mask, cfg)
+            fe = s.step_fn_roeexner(fe, t, d, mask, cfg)
             dts.append(float(d))
+            t += float(d)
         out["fe_dts"] = np.array(dts)
         dump_state("fe", fe, out)
-        # SSPRK2 (intended form)
+        # SSPRK2 (intended form): both stages at the time of the step start
         rk = st
         dts = []
+        t = 0.0
         for _ in range(NSTEPS):
             d = s.compute_dt_roeexner(rk, CFL, mask, cfg)
-            s1 = s.step_fn_roeexner(rk, 0.0, d, mask, cfg)
-            s2 = s.step_fn_roeexner(s1, 0.0, d, mask, cfg)
+            s1 = s.step_fn_roeexner(rk, t, d, mask, cfg)
+            s2 = s.step_fn_roeexner(s1, t, d, mask, cfg)
             rk = ssprk2_average(rk, s2)
             dts.append(float(d))
+            t += float(d)
         out["rk_dts"] = np.array(dts)
         dump_state("rk", rk, out)
         path = os.path.join(HERE, f"re_{name}.npz")

@@ -200,15 +200,27 @@ def test_nonfinite_state_is_reported():
     check_state(st, mask, cfg)  # the flag was cleared by the first check
 
 
-def test_unreachable_boundary_layout_is_rejected():
-    from pyexner_b200._lib import ERR_UNSUPPORTED, PxbError
+def test_inner_boundary_cell_needs_the_general_path():
+    """A boundary polygon around an interior cell: the fused kernel handles ring cells
+    only, so a plan that asks for it is refused; the automatic choice runs the general
+    path and matches the oracle."""
+    from pyexner_b200 import run_steps
+    from pyexner_b200._lib import ERR_UNSUPPORTED, PATH_GENERAL, PxbError
     from pyexner_b200.cases import seds_matrix
+    from pyexner_b200.solvers import _re_plan
 
     arrs, params, X, Y, mpm = random_re_case(20, 24, seed=3)
-    # a boundary polygon around an interior cell: the stage kernels handle ring cells only
     params["boundaries"]["inner"] = {"type": "Transmissive", "polygon": [[9.5, 9.5], [10.5, 9.5], [10.5, 10.5],
                                                                           [9.5, 10.5]],
                                      "values": [0, 0, 0, 0], "normal": [1.0, 0.0]}
+    seds = seds_matrix(params["erosion"])
     with pytest.raises(PxbError) as e:
-        device_re(arrs, params, X, Y, seds_matrix(params["erosion"]), torch.float64, 0.1)
+        device_re(arrs, dict(params, stage_path="fused"), X, Y, seds, torch.float64, 0.1)
     assert e.value.code == ERR_UNSUPPORTED
+    bundle, cfg, mask, st = device_re(arrs, params, X, Y, seds, torch.float64, 0.1)
+    assert _re_plan(st, mask, cfg).path == PATH_GENERAL
+    ost, omask, obcs = oracle_setup(arrs, params, X, Y, mpm, seds)
+    orun, odts = OI.run_roe_exner(ost, omask, obcs, mpm, 0.1, 0.5, 3, "SSPRK2")
+    dts = run_steps(st, mask, cfg, "SSPRK2", 3, 0.5)
+    assert rel_err(dts.cpu().numpy(), odts) <= 1e-10
+    assert_planes(st.to_numpy(), orun, 1e-10, what="inner cell")

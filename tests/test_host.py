@@ -27,11 +27,12 @@ def test_library_exports_every_header_symbol():
 
 
 def test_ctypes_structs_match_header_layout():
-    assert ctypes.sizeof(_lib.BcHandler) == 56
+    assert ctypes.sizeof(_lib.BcHandler) == 120 and _lib.BcHandler.values.offset == 56
     assert ctypes.sizeof(_lib.REFields) == 64
     assert ctypes.sizeof(_lib.RoeFields) == 40
     assert _lib.REConfig.pitch.offset == 8 and _lib.REConfig.dx.offset == 24
-    assert _lib.REConfig.handlers.offset == 56 and ctypes.sizeof(_lib.REConfig) == 72
+    assert _lib.REConfig.handlers.offset == 56 and _lib.REConfig.stage_path.offset == 72
+    assert ctypes.sizeof(_lib.REConfig) == 80
 
 
 @pytest.mark.parametrize("name", sorted(BC_SPECS))

@@ -115,12 +115,21 @@ def test_c_oracle_matches_golden(request, case):
     from oracle import c_oracle as CO
 
     d, bcs, mask, st, mpm = load_re_case(request.config.rootpath, case)
+    if any(hd.kind not in CO.KINDS for hd in bcs.handlers):
+        pytest.skip("the C restatement carries the four boundary types of the benchmark layouts only")
     st = CO.init(st, mask, bcs, mpm, 0.1)
+
+    def close(a, ref, rel, floor):
+        # NaN (nodata beds) in the same places, relative error elsewhere
+        assert np.array_equal(np.isnan(a), np.isnan(ref))
+        ok = ~np.isnan(ref)
+        if ok.any():
+            assert np.max(np.abs(a[ok] - ref[ok])) <= rel * max(floor, np.max(np.abs(ref[ok])))
+
     for k in RE.STATE_FIELDS:
-        assert np.max(np.abs(st[k] - d[f"init_{k}"])) <= 1e-14 * max(1.0, np.max(np.abs(d[f"init_{k}"])))
+        close(st[k], d[f"init_{k}"], 1e-14, 1.0)
     for scheme, tag in (("FE", "fe"), ("SSPRK2", "rk")):
         out, dts = CO.run_roe_exner(st, mask, bcs, mpm, 0.1, 0.5, NSTEPS, scheme)
         assert np.max(np.abs(dts - d[f"{tag}_dts"])) <= 1e-15
         for k in RE.STATE_FIELDS:
-            ref = d[f"{tag}_{k}"]
-            assert np.max(np.abs(out[k] - ref)) <= 1e-13 * max(1e-300, np.max(np.abs(ref))), k
+            close(out[k], d[f"{tag}_{k}"], 1e-13, 1e-300)
