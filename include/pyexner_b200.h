@@ -201,6 +201,52 @@ int pxb_roe_run(pxb_roe_plan* plan, const pxb_roe_fields* a, const pxb_roe_field
                 int32_t scheme, double cfl, void* dt_log, void* stream);
 int pxb_roe_check(pxb_roe_plan* plan, void* stream);
 
+/* --- ragged ensembles ---------------------------------------------------------------- */
+/* No counterpart in the reference (it runs one grid per process).  Many independent
+ * Roe-Exner grids of different sizes advance together: each member has its own state,
+ * boundary handlers and dt (as a separate run of forwardeuler.py:37-49 / SSPRK2.py:30-51
+ * for a fixed step count would), and every phase is one launch for all members (CFL,
+ * stage 1, stage 2), the steps captured into a CUDA graph.  Members run the fused stage
+ * kernel, so their layouts must be ones it accepts (PXB_ERR_UNSUPPORTED otherwise).
+ * All members share dtype, the grass-factor mode and the sediment table. */
+typedef struct pxb_re_member {
+    int32_t ny, nx;
+    int64_t pitch;
+    double dx;
+    pxb_re_fields a;                 /* state, advanced in place                        */
+    pxb_re_fields b;                 /* scratch state of the same layout (h, hu, hv, z_b, G) */
+    const uint8_t* nodata;           /* device mask[0] plane or NULL                    */
+    const pxb_bc_handler* handlers;  /* host array, YAML order                          */
+    int32_t nhandlers;
+} pxb_re_member;
+
+typedef struct pxb_re_ens_config {
+    int32_t dtype;
+    int32_t mpm;
+    const double* seds;              /* 7 x nsed, as pxb_re_config                      */
+    int32_t nsed;
+    const pxb_re_member* members;    /* host array                                      */
+    int32_t nmembers;
+    int32_t band_rows;               /* rows per band for every member; 0 = default     */
+} pxb_re_ens_config;
+
+typedef struct pxb_re_ens pxb_re_ens;
+
+int pxb_re_ens_create(const pxb_re_ens_config* cfg, pxb_re_ens** out);
+int pxb_re_ens_destroy(pxb_re_ens* ens);
+/* init_fn_roeexner on every member's state a. */
+int pxb_re_ens_init(pxb_re_ens* ens, void* stream);
+/* Times the ensemble stage kernel for a set of band heights on the current states
+ * (stage 1 from a into b; the states a are left unchanged), keeps the fastest and
+ * returns it in *band_rows (may be NULL).  Synchronises `stream`. */
+int pxb_re_ens_autotune(pxb_re_ens* ens, void* stream, int32_t* band_rows);
+/* nsteps steps of every member (scheme PXB_FE / PXB_SSPRK2), states start and end in a.
+ * dt_log: device array of nsteps x nmembers dts (member index fastest) or NULL. */
+int pxb_re_ens_run(pxb_re_ens* ens, int32_t nsteps, int32_t scheme, double cfl, void* dt_log, void* stream);
+/* Reads and clears the members' error words; *first_bad is the first member that saw a
+ * non-finite dt or state (-1 if none).  Returns PXB_OK or PXB_ERR_NONFINITE. */
+int pxb_re_ens_check(pxb_re_ens* ens, void* stream, int32_t* first_bad);
+
 /* --- allocation-free time step ----------------------------------------------------- */
 /* No counterpart in the reference: PyExner's JAX step never manages device memory
  * itself.  For callers that cannot allocate device memory when they need dt -- an XLA

@@ -85,6 +85,32 @@ class RoeConfig(ctypes.Structure):
     ]
 
 
+class REMember(ctypes.Structure):
+    _fields_ = [
+        ("ny", c_int32),
+        ("nx", c_int32),
+        ("pitch", c_int64),
+        ("dx", c_double),
+        ("a", REFields),
+        ("b", REFields),
+        ("nodata", c_void_p),
+        ("handlers", POINTER(BcHandler)),
+        ("nhandlers", c_int32),
+    ]
+
+
+class REEnsConfig(ctypes.Structure):
+    _fields_ = [
+        ("dtype", c_int32),
+        ("mpm", c_int32),
+        ("seds", c_void_p),
+        ("nsed", c_int32),
+        ("members", POINTER(REMember)),
+        ("nmembers", c_int32),
+        ("band_rows", c_int32),
+    ]
+
+
 class PxbError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"pyexner_b200 error {code}: {msg}")
@@ -111,6 +137,12 @@ SIGNATURES = {
     "pxb_roe_stage": [c_void_p, POINTER(RoeFields), POINTER(RoeFields), POINTER(RoeFields), c_void_p, c_void_p],
     "pxb_roe_run": [c_void_p, POINTER(RoeFields), POINTER(RoeFields), c_int32, c_int32, c_double, c_void_p, c_void_p],
     "pxb_roe_check": [c_void_p, c_void_p],
+    "pxb_re_ens_create": [POINTER(REEnsConfig), POINTER(c_void_p)],
+    "pxb_re_ens_destroy": [c_void_p],
+    "pxb_re_ens_init": [c_void_p, c_void_p],
+    "pxb_re_ens_autotune": [c_void_p, c_void_p, POINTER(c_int32)],
+    "pxb_re_ens_run": [c_void_p, c_int32, c_int32, c_double, c_void_p, c_void_p],
+    "pxb_re_ens_check": [c_void_p, c_void_p, POINTER(c_int32)],
     "pxb_re_cfl_noalloc": [c_int32, c_int32, c_int64, c_int32, c_double, c_double, c_void_p, c_void_p, c_void_p,
                            c_void_p, c_void_p, c_void_p, c_void_p],
     "pxb_version": [],

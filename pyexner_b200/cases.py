@@ -53,10 +53,24 @@ def gaussian_bed_fields(n, dx=0.01, seed_bed=1, seed_noise=2, device=None):
     With ``device`` set (e.g. "cuda") the bed sum is evaluated with torch on that device,
     which is what makes the 8192^2 case quick to build; the numbers are the same
     float64 expression either way."""
-    ny = nx = n + 2
-    L = n * dx
+    zt = gaussian_bed_total(n, n, dx, seed_bed, device)
+    z = np.full(zt.shape, zt.min() - 0.05)
+    zb = zt - z
+    rn = np.random.default_rng(seed_noise)
+    noise = rn.uniform(-1.0, 1.0, zt.shape)
+    h = np.maximum(0.0, (0.3 - zt) * (1.0 + 0.02 * noise))
+    return dict(h=h, hu=0.1 * h, hv=np.zeros_like(h), z=z, z_b=zb, n=np.zeros_like(h), G=np.zeros_like(h))
+
+
+def gaussian_bed_total(ny_phys, nx_phys, dx=0.01, seed_bed=1, device=None):
+    """z_t = 0.05 sum_k A_k exp(-|x - c_k|^2 / (2 s_k^2)) on the (ny+2, nx+2) grid with
+    ring: c_k ~ U(domain), s_k ~ U(0.05, 0.3) L with L = sqrt(Lx Ly) (the side of a square
+    domain), A_k ~ U(-1, 1)."""
+    ny, nx = ny_phys + 2, nx_phys + 2
+    Lx, Ly = nx_phys * dx, ny_phys * dx
+    L = float(np.sqrt(Lx * Ly))
     rb = np.random.default_rng(seed_bed)
-    ck = rb.uniform(0.0, L, (16, 2))
+    ck = rb.uniform(0.0, 1.0, (16, 2)) * np.array([Lx, Ly])
     sk = rb.uniform(0.05, 0.3, 16) * L
     ak = rb.uniform(-1.0, 1.0, 16)
     xc = (np.arange(nx) - 0.5) * dx
@@ -79,12 +93,7 @@ def gaussian_bed_fields(n, dx=0.01, seed_bed=1, seed_noise=2, device=None):
             gy = torch.exp(-((ty - ck[k, 1]) ** 2) / (2 * sk[k] ** 2))
             acc += ak[k] * torch.outer(gy, gx)
         zt = (0.05 * acc).cpu().numpy()
-    z = np.full((ny, nx), zt.min() - 0.05)
-    zb = zt - z
-    rn = np.random.default_rng(seed_noise)
-    noise = rn.uniform(-1.0, 1.0, (ny, nx))
-    h = np.maximum(0.0, (0.3 - zt) * (1.0 + 0.02 * noise))
-    return dict(h=h, hu=0.1 * h, hv=np.zeros_like(h), z=z, z_b=zb, n=np.zeros_like(h), G=np.zeros_like(h))
+    return zt
 
 
 def gaussian_bed(n, dx=0.01, seed_bed=1, seed_noise=2, device=None):
@@ -148,3 +157,41 @@ def berthon_case(dh=0.1, end_time=10.0, out_freq=1.0, integrator="Forward Euler"
         ),
     )
     return x, y, fields, params
+
+
+# ------------------------------------------------------------------ ragged ensemble
+def ensemble_fields(ny_phys, nx_phys, step_height, dx=0.01, seed_bed=1):
+    """One member of the ragged dam-break ensemble: the Gaussian-sum bed of
+    ``gaussian_bed_total`` on an ny x nx grid (split into a constant rigid bed 5 cm below
+    its minimum and the erodible layer above it), water at rest at
+    h = max(0, 0.3 - z_t) + H [x < Lx / 2]."""
+    zt = gaussian_bed_total(ny_phys, nx_phys, dx, seed_bed)
+    z = np.full(zt.shape, zt.min() - 0.05)
+    zb = zt - z
+    xc = (np.arange(nx_phys + 2) - 0.5) * dx
+    h = np.maximum(0.0, 0.3 - zt) + step_height * (xc[None, :] < 0.5 * nx_phys * dx)
+    zeros = np.zeros_like(h)
+    return dict(h=h, hu=zeros.copy(), hv=zeros.copy(), z=z, z_b=zb, n=zeros.copy(), G=zeros.copy())
+
+
+def ensemble_case(count=64, seed=0, sides=(128, 1024), heights=(0.2, 1.0), dx=0.01):
+    """The ragged ensemble workload: ``count`` Roe-Exner dam breaks whose grid sides are
+    drawn independently from U{sides} (seeded, non-square allowed), each with its own
+    Gaussian-sum bed (seed ``1000 * seed + k``) and its own step height H ~ U(heights);
+    MPM with one sediment, Transmissive + TransmissiveBed in x, Reflective in y.
+
+    Returns (members, erosion): ``members`` holds per member ``arrs`` (float64 planes with
+    the ring), ``shape``, ``height``, ``dx`` and the YAML-style ``params``."""
+    rs = np.random.default_rng(seed)
+    erosion = dict(grass_factor="MPM", bulk_porosity=0.42, sediments=SED_ONE)
+    members = []
+    for k in range(count):
+        nyp, nxp = (int(v) for v in rs.integers(sides[0], sides[1] + 1, 2))
+        H = float(rs.uniform(heights[0], heights[1]))
+        arrs = ensemble_fields(nyp, nxp, H, dx, seed_bed=1000 * seed + k)
+        ny, nx = nyp + 2, nxp + 2
+        bspec = ring_boundaries(ny, nx, ["Transmissive", "TransmissiveBed"], ["Transmissive", "TransmissiveBed"],
+                                ["Reflective"], ["Reflective"])
+        params = dict(flux_scheme="Roe Exner", integrator="SSPRK2", cfl=0.5, erosion=erosion, boundaries=bspec)
+        members.append(dict(arrs=arrs, shape=(ny, nx), height=H, dx=dx, params=params))
+    return members, erosion

@@ -558,6 +558,79 @@ struct pxb_roe_plan {
     PlanCommon c;
 };
 
+// One member of a ragged ensemble.
+struct EnsMember {
+    int ny = 0, nx = 0;
+    long long pitch = 0;
+    double dx = 0;
+    pxb_re_fields a{}, b{};
+    const uint8_t* nodata = nullptr;
+    pxb_ring_recipe* ring = nullptr;  // device, null without handlers
+    std::vector<DevHandler> handlers;
+};
+
+struct pxb_re_ens {
+    int dtype = 0, mpm = 0, nm = 0;
+    int band_rows = 0;
+    int sm_count = 0;
+    int bps[2] = {1, 1};  // resident stage blocks per SM: plain, averaged
+    bool has_mask = false;
+    std::vector<EnsMember> m;
+    std::vector<void*> owned;           // zero nodata planes of members without one
+    void* bc_tmp = nullptr;
+    pxb::SedTable<float> sedf;
+    pxb::SedTable<double> sedd;
+    pxb::CflScratch* scr = nullptr;     // one per member
+    void* dt = nullptr;                 // one dt per member (dtype)
+    // argument tables on the device: stage 0 a->b, 1 b->a, 2 b->a averaged with a, 3 a->b without G;
+    // CFL 0 on a, 1 on b
+    void* st_args[4] = {nullptr, nullptr, nullptr, nullptr};
+    void* cfl_args[2] = {nullptr, nullptr};
+    int* st_base = nullptr;
+    int* cfl_base = nullptr;
+    int st_total = 0, cfl_total = 0;
+    double cfl_value = -1;
+    const void* cfl_log = nullptr;
+    cudaStream_t cap = nullptr;
+    struct Cached {
+        std::vector<const void*> key;
+        cudaGraphExec_t exec = nullptr;
+    };
+    std::vector<Cached> graphs;
+
+    size_t esize() const { return dtype == PXB_F64 ? 8 : 4; }
+    void drop_graphs() {
+        for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
+        graphs.clear();
+    }
+    void release() {
+        drop_graphs();
+        for (auto& mb : m) {
+            for (auto& h : mb.handlers) {
+                cudaFree(h.cells);
+                cudaFree(h.donors);
+            }
+            cudaFree(mb.ring);
+        }
+        m.clear();
+        for (void* p : owned) cudaFree(p);
+        owned.clear();
+        for (auto& p : st_args) cudaFree(p), p = nullptr;
+        for (auto& p : cfl_args) cudaFree(p), p = nullptr;
+        cudaFree(st_base);
+        cudaFree(cfl_base);
+        cudaFree(bc_tmp);
+        cudaFree(scr);
+        cudaFree(dt);
+        if (cap) cudaStreamDestroy(cap);
+        st_base = cfl_base = nullptr;
+        bc_tmp = nullptr;
+        scr = nullptr;
+        dt = nullptr;
+        cap = nullptr;
+    }
+};
+
 namespace {
 
 template <class T>
@@ -642,8 +715,9 @@ int re_stage_impl(pxb_re_plan* P, const pxb_re_fields* in, const pxb_re_fields* 
 // Every handler in order on the field slots f (h, hu, hv, z_b, n, G), at the time *tptr
 // (device) or tval.
 template <class T>
-int apply_handlers(PlanCommon& C, T* const f[6], const double* tptr, double tval, cudaStream_t s) {
-    for (auto& h : C.handlers) {
+int apply_handlers(const std::vector<DevHandler>& hs, void* bc_tmp, T* const f[6], const double* tptr, double tval,
+                   cudaStream_t s) {
+    for (auto& h : hs) {
         pxb::BcArgs<T> b{};
         for (int k = 0; k < 6; ++k) b.f[k] = f[k];
         b.cells = h.cells;
@@ -662,10 +736,38 @@ int apply_handlers(PlanCommon& C, T* const f[6], const double* tptr, double tval
         b.hb = (T)h.hb;
         b.tptr = tptr;
         b.tval = tval;
-        b.tmp = (T*)C.bc_tmp;
+        b.tmp = (T*)bc_tmp;
         PXB_CUDA(pxb::launch_bc<T>(b, s));
     }
     return PXB_OK;
+}
+
+template <class T>
+int apply_handlers(PlanCommon& C, T* const f[6], const double* tptr, double tval, cudaStream_t s) {
+    return apply_handlers<T>(C.handlers, C.bc_tmp, f, tptr, tval, s);
+}
+
+// init_fn_roeexner on one grid: n_b and G, then the handlers at t = 0.
+template <class T>
+int init_fields(int ny, int nx, long long pitch, const pxb_re_fields* f, const uint8_t* nodata, int mpm,
+                const pxb::SedTable<T>& sed, const std::vector<DevHandler>& hs, void* bc_tmp, cudaStream_t s) {
+    pxb::InitArgs<T> a{};
+    a.ny = ny;
+    a.nx = nx;
+    a.pitch = pitch;
+    a.h = (const T*)f->h;
+    a.hu = (const T*)f->hu;
+    a.hv = (const T*)f->hv;
+    a.zb = (const T*)f->z_b;
+    a.n = (const T*)f->n;
+    a.nb = (T*)f->n_b;
+    a.G = (T*)f->G;
+    a.nodata = nodata;
+    a.mpm = mpm;
+    a.sed = sed;
+    PXB_CUDA(pxb::launch_re_init<T>(a, s));
+    T* const fs[6] = {(T*)f->h, (T*)f->hu, (T*)f->hv, (T*)f->z_b, (T*)f->n, (T*)f->G};
+    return apply_handlers<T>(hs, bc_tmp, fs, nullptr, 0.0, s);
 }
 
 // One stage on the general path (re_general.cuh).
@@ -730,23 +832,8 @@ int re_general_impl(pxb_re_plan* P, const pxb_re_fields* in, const pxb_re_fields
 
 template <class T>
 int re_init_impl(pxb_re_plan* P, const pxb_re_fields* f, cudaStream_t s) {
-    pxb::InitArgs<T> a{};
-    a.ny = P->c.ny;
-    a.nx = P->c.nx;
-    a.pitch = P->c.pitch;
-    a.h = (const T*)f->h;
-    a.hu = (const T*)f->hu;
-    a.hv = (const T*)f->hv;
-    a.zb = (const T*)f->z_b;
-    a.n = (const T*)f->n;
-    a.nb = (T*)f->n_b;
-    a.G = (T*)f->G;
-    a.nodata = P->nodata;
-    a.mpm = P->mpm;
-    a.sed = sed_of<T>(P);
-    PXB_CUDA(pxb::launch_re_init<T>(a, s));
-    T* const fs[6] = {(T*)f->h, (T*)f->hu, (T*)f->hv, (T*)f->z_b, (T*)f->n, (T*)f->G};
-    return apply_handlers<T>(P->c, fs, nullptr, 0.0, s);
+    return init_fields<T>(P->c.ny, P->c.nx, P->c.pitch, f, P->nodata, P->mpm, sed_of<T>(P), P->c.handlers,
+                          P->c.bc_tmp, s);
 }
 
 // One stage on the plan's path; the general path reads the time from *tptr or tval.
@@ -880,6 +967,258 @@ int check_roe_fields(const pxb_roe_fields* f) {
     return PXB_OK;
 }
 
+// ------------------------------------------------------------------ ragged ensembles
+template <class T>
+const pxb::SedTable<T>& ens_sed(const pxb_re_ens* E);
+template <>
+const pxb::SedTable<float>& ens_sed<float>(const pxb_re_ens* E) { return E->sedf; }
+template <>
+const pxb::SedTable<double>& ens_sed<double>(const pxb_re_ens* E) { return E->sedd; }
+
+constexpr int ENS_CFL_ROWS = 32;  // rows per CFL work item
+
+template <class T>
+pxb::REStageArgs<T> ens_stage_args(const pxb_re_ens* E, int k, const pxb_re_fields* in, const pxb_re_fields* out,
+                                   const pxb_re_fields* avg, const pxb_re_fields* statics) {
+    const EnsMember& mb = E->m[(size_t)k];
+    pxb::REStageArgs<T> a{};
+    a.ny = mb.ny;
+    a.nx = mb.nx;
+    a.pitch = mb.pitch;
+    a.dx = (T)mb.dx;
+    a.h = (const T*)in->h;
+    a.hu = (const T*)in->hu;
+    a.hv = (const T*)in->hv;
+    a.zb = (const T*)in->z_b;
+    a.z = (const T*)statics->z;
+    a.nb = (const T*)statics->n_b;
+    a.G = (const T*)in->G;
+    a.nodata = mb.nodata;
+    a.oh = (T*)out->h;
+    a.ohu = (T*)out->hu;
+    a.ohv = (T*)out->hv;
+    a.ozb = (T*)out->z_b;
+    a.oG = (T*)out->G;
+    if (avg) {
+        a.ah = (const T*)avg->h;
+        a.ahu = (const T*)avg->hu;
+        a.ahv = (const T*)avg->hv;
+        a.azb = (const T*)avg->z_b;
+        a.aG = (const T*)avg->G;
+    }
+    a.dt = (const T*)E->dt + k;
+    a.ring = mb.ring;
+    a.sed = ens_sed<T>(E);
+    a.band_rows = E->band_rows;
+    a.nstrips = std::max(1, (mb.nx - 3 + PXB_STRIP_OUT - 1) / PXB_STRIP_OUT);
+    a.nbands = std::max(1, (mb.ny - 1 + E->band_rows - 1) / E->band_rows);
+    a.err = &E->scr[k].err;
+    return a;
+}
+
+// Stage argument tables and item offsets for the current band height.
+template <class T>
+int ens_build_stage_tables(pxb_re_ens* E) {
+    std::vector<pxb::REStageArgs<T>> t[4];
+    std::vector<int> base(1, 0);
+    for (int k = 0; k < E->nm; ++k) {
+        const EnsMember& mb = E->m[(size_t)k];
+        pxb_re_fields b_noG = mb.b;  // SSPRK2 stage 1 in MPM mode: G is recomputed by stage 2
+        b_noG.G = nullptr;
+        t[0].push_back(ens_stage_args<T>(E, k, &mb.a, &mb.b, nullptr, &mb.a));
+        t[1].push_back(ens_stage_args<T>(E, k, &mb.b, &mb.a, nullptr, &mb.a));
+        t[2].push_back(ens_stage_args<T>(E, k, &mb.b, &mb.a, &mb.a, &mb.a));
+        t[3].push_back(ens_stage_args<T>(E, k, &mb.a, &b_noG, nullptr, &mb.a));
+        const pxb::REStageArgs<T>& a = t[0].back();
+        base.push_back(base.back() + a.nstrips * a.nbands);
+    }
+    for (int v = 0; v < 4; ++v) {
+        if (!E->st_args[v]) PXB_CUDA(cudaMalloc(&E->st_args[v], sizeof(pxb::REStageArgs<T>) * E->nm));
+        PXB_CUDA(cudaMemcpy(E->st_args[v], t[v].data(), sizeof(pxb::REStageArgs<T>) * E->nm, cudaMemcpyHostToDevice));
+    }
+    if (!E->st_base) PXB_CUDA(cudaMalloc(&E->st_base, sizeof(int) * (E->nm + 1)));
+    PXB_CUDA(cudaMemcpy(E->st_base, base.data(), sizeof(int) * (E->nm + 1), cudaMemcpyHostToDevice));
+    E->st_total = base.back();
+    E->drop_graphs();
+    return PXB_OK;
+}
+
+// CFL argument tables for a cfl number and a dt log.
+template <class T>
+int ens_build_cfl_tables(pxb_re_ens* E, double cfl, void* dt_log) {
+    std::vector<pxb::CflArgs<T>> t[2];
+    std::vector<int> base(1, 0);
+    for (int k = 0; k < E->nm; ++k) {
+        const EnsMember& mb = E->m[(size_t)k];
+        for (int v = 0; v < 2; ++v) {
+            const pxb_re_fields& f = v == 0 ? mb.a : mb.b;
+            pxb::CflArgs<T> a{};
+            a.ny = mb.ny;
+            a.nx = mb.nx;
+            a.pitch = mb.pitch;
+            a.h = (const T*)f.h;
+            a.hu = (const T*)f.hu;
+            a.hv = (const T*)f.hv;
+            a.G = (const T*)f.G;
+            a.nodata = mb.nodata;
+            a.dx = (T)mb.dx;
+            a.cfl = (T)cfl;
+            a.floor_dt = (T)pxb::DT_FLOOR;
+            a.scr = E->scr + k;
+            a.dt_out = (T*)E->dt + k;
+            a.dt_log = (T*)dt_log;
+            a.band_rows = ENS_CFL_ROWS;
+            a.nstrips = std::max(1, (mb.nx + 30) / 31);
+            a.nbands = std::max(1, (mb.ny + ENS_CFL_ROWS - 1) / ENS_CFL_ROWS);
+            t[v].push_back(a);
+        }
+        base.push_back(base.back() + t[0].back().nstrips * t[0].back().nbands);
+    }
+    for (int v = 0; v < 2; ++v) {
+        if (!E->cfl_args[v]) PXB_CUDA(cudaMalloc(&E->cfl_args[v], sizeof(pxb::CflArgs<T>) * E->nm));
+        PXB_CUDA(cudaMemcpy(E->cfl_args[v], t[v].data(), sizeof(pxb::CflArgs<T>) * E->nm, cudaMemcpyHostToDevice));
+    }
+    if (!E->cfl_base) PXB_CUDA(cudaMalloc(&E->cfl_base, sizeof(int) * (E->nm + 1)));
+    PXB_CUDA(cudaMemcpy(E->cfl_base, base.data(), sizeof(int) * (E->nm + 1), cudaMemcpyHostToDevice));
+    E->cfl_total = base.back();
+    E->cfl_value = cfl;
+    E->cfl_log = dt_log;
+    E->drop_graphs();
+    return PXB_OK;
+}
+
+template <class T>
+int ens_stage_launch(pxb_re_ens* E, int v, cudaStream_t s) {
+    pxb::EnsStageArgs<T> a{};
+    a.args = (const pxb::REStageArgs<T>*)E->st_args[v];
+    a.base = E->st_base;
+    a.nmembers = E->nm;
+    const bool avg = v == 2;
+    const int grid = std::max(1, std::min((E->st_total + 3) / 4, std::max(1, E->bps[avg ? 1 : 0]) * E->sm_count));
+    PXB_CUDA(pxb::launch_ens_stage<T>(a, E->mpm != 0, E->has_mask, avg, grid, s));
+    return PXB_OK;
+}
+
+template <class T>
+int ens_cfl_launch(pxb_re_ens* E, int v, cudaStream_t s) {
+    pxb::EnsCflArgs<T> a{};
+    a.args = (const pxb::CflArgs<T>*)E->cfl_args[v];
+    a.base = E->cfl_base;
+    a.nmembers = E->nm;
+    a.log_stride = E->nm;
+    const int grid = std::max(1, std::min((E->cfl_total + 7) / 8, 8 * E->sm_count));
+    PXB_CUDA(pxb::launch_ens_cfl<T>(a, E->has_mask, grid, s));
+    return PXB_OK;
+}
+
+template <class T>
+int ens_run_impl(pxb_re_ens* E, int nsteps, int scheme, double cfl, void* dt_log, cudaStream_t s) {
+    if (cfl != E->cfl_value || dt_log != E->cfl_log) {
+        const int st = ens_build_cfl_tables<T>(E, cfl, dt_log);
+        if (st != PXB_OK) return st;
+    }
+    // the dt log restarts at row 0
+    PXB_CUDA(cudaMemset2DAsync(&E->scr[0].step, sizeof(pxb::CflScratch), 0, sizeof(unsigned int), E->nm, s));
+    std::vector<const void*> key = {(const void*)(intptr_t)scheme, (const void*)(intptr_t)E->band_rows};
+    auto body_rk = [&](cudaStream_t st) {
+        int r = ens_cfl_launch<T>(E, 0, st);
+        if (r == PXB_OK) r = ens_stage_launch<T>(E, E->mpm ? 3 : 0, st);
+        if (r == PXB_OK) r = ens_stage_launch<T>(E, 2, st);
+        return r;
+    };
+    auto body_fe2 = [&](cudaStream_t st) {
+        int r = ens_cfl_launch<T>(E, 0, st);
+        if (r == PXB_OK) r = ens_stage_launch<T>(E, 0, st);
+        if (r == PXB_OK) r = ens_cfl_launch<T>(E, 1, st);
+        if (r == PXB_OK) r = ens_stage_launch<T>(E, 1, st);
+        return r;
+    };
+    const int reps = scheme == PXB_SSPRK2 ? nsteps : nsteps / 2;
+    if (reps > 0) {
+        cudaGraphExec_t exec = nullptr;
+        for (auto& g : E->graphs)
+            if (g.key == key) exec = g.exec;
+        if (!exec) {
+            PXB_CUDA(cudaStreamBeginCapture(E->cap, cudaStreamCaptureModeThreadLocal));
+            const int st = scheme == PXB_SSPRK2 ? body_rk(E->cap) : body_fe2(E->cap);
+            cudaGraph_t graph = nullptr;
+            const cudaError_t ec = cudaStreamEndCapture(E->cap, &graph);
+            if (st != PXB_OK) {
+                if (graph) cudaGraphDestroy(graph);
+                return st;
+            }
+            if (ec != cudaSuccess) return fail(PXB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
+            const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (ei != cudaSuccess) return fail(PXB_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+            pxb_re_ens::Cached c;
+            c.key = key;
+            c.exec = exec;
+            E->graphs.push_back(c);
+        }
+        for (int i = 0; i < reps; ++i) PXB_CUDA(cudaGraphLaunch(exec, s));
+    }
+    if (scheme == PXB_SSPRK2 || (nsteps & 1) == 0) return PXB_OK;
+    // odd Forward-Euler step: a -> b, then b back into a
+    int r = ens_cfl_launch<T>(E, 0, s);
+    if (r == PXB_OK) r = ens_stage_launch<T>(E, 0, s);
+    if (r != PXB_OK) return r;
+    const size_t es = E->esize();
+    for (const EnsMember& mb : E->m) {
+        const void* src[5] = {mb.b.h, mb.b.hu, mb.b.hv, mb.b.z_b, mb.b.G};
+        void* dst[5] = {mb.a.h, mb.a.hu, mb.a.hv, mb.a.z_b, mb.a.G};
+        for (int k = 0; k < 5; ++k)
+            PXB_CUDA(cudaMemcpy2DAsync(dst[k], mb.pitch * es, src[k], mb.pitch * es, mb.nx * es, mb.ny,
+                                       cudaMemcpyDeviceToDevice, s));
+    }
+    return PXB_OK;
+}
+
+// Candidate band heights timed on stage 1 (a -> b) of the current states; keeps the fastest.
+template <class T>
+int ens_autotune_impl(pxb_re_ens* E, cudaStream_t s, int32_t* out) {
+    static const int cand[] = {8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256};
+    int st = ens_build_cfl_tables<T>(E, 0.5, nullptr);
+    if (st != PXB_OK) return st;
+    st = ens_cfl_launch<T>(E, 0, s);  // a dt to run the stage with (the states are not touched)
+    if (st != PXB_OK) return st;
+    cudaEvent_t e0, e1;
+    PXB_CUDA(cudaEventCreate(&e0));
+    PXB_CUDA(cudaEventCreate(&e1));
+    float best_ms = 1e30f;
+    int best = E->band_rows;
+    for (int rows : cand) {
+        E->band_rows = rows;
+        st = ens_build_stage_tables<T>(E);
+        if (st == PXB_OK) st = ens_stage_launch<T>(E, 0, s);  // warm-up
+        float ms = 1e30f;
+        for (int rep = 0; rep < 3 && st == PXB_OK; ++rep) {
+            cudaEventRecord(e0, s);
+            st = ens_stage_launch<T>(E, 0, s);
+            cudaEventRecord(e1, s);
+            cudaEventSynchronize(e1);
+            float t = 0;
+            cudaEventElapsedTime(&t, e0, e1);
+            ms = std::min(ms, t);
+        }
+        if (st != PXB_OK) break;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = rows;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != PXB_OK) return st;
+    E->band_rows = best;
+    st = ens_build_stage_tables<T>(E);
+    if (st != PXB_OK) return st;
+    PXB_CUDA(cudaMemset2DAsync(&E->scr[0].step, sizeof(pxb::CflScratch), 0, sizeof(unsigned int), E->nm, s));
+    PXB_CUDA(cudaStreamSynchronize(s));
+    if (out) *out = best;
+    return PXB_OK;
+}
+
 }  // namespace
 
 // ===================================================================== C entry points
@@ -991,6 +1330,159 @@ int pxb_re_run(pxb_re_plan* P, const pxb_re_fields* a, const pxb_re_fields* b, i
 int pxb_re_check(pxb_re_plan* P, void* stream) {
     if (!P) return fail(PXB_ERR_ARG, "null plan");
     return check_plan_error(P->c, (cudaStream_t)stream);
+}
+
+int pxb_re_ens_create(const pxb_re_ens_config* cfg, pxb_re_ens** out) {
+    if (!cfg || !out) return fail(PXB_ERR_ARG, "null config or output pointer");
+    *out = nullptr;
+    if (cfg->nmembers < 1 || !cfg->members) return fail(PXB_ERR_ARG, "an ensemble needs at least one member");
+    if (cfg->dtype != PXB_F32 && cfg->dtype != PXB_F64) return fail(PXB_ERR_ARG, "dtype must be PXB_F32 or PXB_F64");
+    if (cfg->mpm && (!cfg->seds || cfg->nsed < 1 || cfg->nsed > PXB_MAX_SED))
+        return fail(PXB_ERR_ARG, "MPM needs 1..8 sediment classes");
+    if (cfg->band_rows < 0) return fail(PXB_ERR_ARG, "band_rows < 0");
+    pxb_re_ens* E = new pxb_re_ens();
+    auto bail = [&](int code) {
+        E->release();
+        delete E;
+        return code;
+    };
+    E->dtype = cfg->dtype;
+    E->mpm = cfg->mpm;
+    E->nm = cfg->nmembers;
+    E->band_rows = cfg->band_rows > 0 ? cfg->band_rows : 64;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&E->sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return bail(fail(PXB_ERR_CUDA, "no CUDA device"));
+    if (cfg->mpm) {
+        fill_sed(E->sedf, cfg->seds, cfg->nsed);
+        fill_sed(E->sedd, cfg->seds, cfg->nsed);
+    }
+    const size_t es = E->esize();
+    int maxcount = 0;
+    for (int k = 0; k < E->nm; ++k) {
+        const pxb_re_member& M = cfg->members[k];
+        const std::string who = "member " + std::to_string(k) + ": ";
+        if (M.ny < 3 || M.nx < 3) return bail(fail(PXB_ERR_ARG, who + "grid must be at least 3 x 3 cells"));
+        if (M.pitch < M.nx) return bail(fail(PXB_ERR_ARG, who + "pitch smaller than nx"));
+        if ((long long)M.ny * M.pitch >= (1LL << 31)) return bail(fail(PXB_ERR_ARG, who + "plane of 2^31 elements or more"));
+        if (!(M.dx > 0) || !std::isfinite(M.dx)) return bail(fail(PXB_ERR_ARG, who + "dx must be positive and finite"));
+        if (!M.a.h || !M.a.hu || !M.a.hv || !M.a.z || !M.a.z_b || !M.a.n || !M.a.n_b || !M.a.G)
+            return bail(fail(PXB_ERR_ARG, who + "every plane of a must be set"));
+        if (!M.b.h || !M.b.hu || !M.b.hv || !M.b.z_b || !M.b.G)
+            return bail(fail(PXB_ERR_ARG, who + "b needs h, hu, hv, z_b and G"));
+        if (M.nhandlers < 0 || (M.nhandlers > 0 && !M.handlers)) return bail(fail(PXB_ERR_ARG, who + "null handlers"));
+        EnsMember mb;
+        mb.ny = M.ny;
+        mb.nx = M.nx;
+        mb.pitch = M.pitch;
+        mb.dx = M.dx;
+        mb.a = M.a;
+        mb.b = M.b;
+        mb.nodata = M.nodata;
+        E->has_mask = E->has_mask || M.nodata != nullptr;
+        for (int q = 0; q < M.nhandlers; ++q)
+            if (!kind_ok(M.handlers[q].kind, false))
+                return bail(fail(PXB_ERR_ARG, who + "handler " + std::to_string(q) + " is not a \"Roe Exner\" handler"));
+        if (M.nhandlers > 0) {
+            Resolved R = resolve(M.handlers, M.nhandlers, M.ny, M.nx, M.pitch, false, true);
+            if (!R.error.empty()) return bail(fail(PXB_ERR_UNSUPPORTED, who + R.error));
+            int mc = 0;
+            const int st = upload_handlers(M.handlers, M.nhandlers, (long long)(M.ny - 1) * M.pitch + M.nx, mb.handlers, mc);
+            E->m.push_back(mb);  // owned from here on (released with the ensemble)
+            if (st != PXB_OK) return bail(st);
+            maxcount = std::max(maxcount, mc);
+            EnsMember& me = E->m.back();
+            if (cudaMalloc(&me.ring, sizeof(pxb_ring_recipe) * R.ring.size()) != cudaSuccess ||
+                cudaMemcpy(me.ring, R.ring.data(), sizeof(pxb_ring_recipe) * R.ring.size(), cudaMemcpyHostToDevice) !=
+                    cudaSuccess)
+                return bail(fail(PXB_ERR_CUDA, who + "ring recipes"));
+        } else {
+            E->m.push_back(mb);
+        }
+    }
+    if (E->has_mask) {  // members without a mask read a zero plane
+        for (auto& mb : E->m) {
+            if (mb.nodata) continue;
+            void* p = nullptr;
+            const size_t bytes = (size_t)mb.ny * (size_t)mb.pitch;
+            if (cudaMalloc(&p, bytes) != cudaSuccess || cudaMemset(p, 0, bytes) != cudaSuccess)
+                return bail(fail(PXB_ERR_CUDA, "nodata plane"));
+            E->owned.push_back(p);
+            mb.nodata = (const uint8_t*)p;
+        }
+    }
+    if (cudaMalloc(&E->bc_tmp, 6 * (size_t)std::max(1, maxcount) * es) != cudaSuccess ||
+        cudaMalloc(&E->scr, sizeof(pxb::CflScratch) * E->nm) != cudaSuccess ||
+        cudaMemset(E->scr, 0, sizeof(pxb::CflScratch) * E->nm) != cudaSuccess ||
+        cudaMalloc(&E->dt, es * E->nm) != cudaSuccess || cudaMemset(E->dt, 0, es * E->nm) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&E->cap, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(PXB_ERR_CUDA, "ensemble scratch"));
+    for (int v = 0; v < 2; ++v)
+        E->bps[v] = E->dtype == PXB_F64 ? pxb::ens_stage_blocks_per_sm<double>(E->mpm != 0, E->has_mask, v == 1)
+                                        : pxb::ens_stage_blocks_per_sm<float>(E->mpm != 0, E->has_mask, v == 1);
+    int st = E->dtype == PXB_F64 ? ens_build_stage_tables<double>(E) : ens_build_stage_tables<float>(E);
+    if (st != PXB_OK) return bail(st);
+    *out = E;
+    return PXB_OK;
+}
+
+int pxb_re_ens_destroy(pxb_re_ens* E) {
+    if (!E) return PXB_OK;
+    cudaDeviceSynchronize();
+    E->release();
+    delete E;
+    return PXB_OK;
+}
+
+int pxb_re_ens_init(pxb_re_ens* E, void* stream) {
+    if (!E) return fail(PXB_ERR_ARG, "null ensemble");
+    cudaStream_t s = (cudaStream_t)stream;
+    for (const EnsMember& mb : E->m) {
+        const int st = E->dtype == PXB_F64
+                           ? init_fields<double>(mb.ny, mb.nx, mb.pitch, &mb.a, mb.nodata, E->mpm, E->sedd, mb.handlers,
+                                                 E->bc_tmp, s)
+                           : init_fields<float>(mb.ny, mb.nx, mb.pitch, &mb.a, mb.nodata, E->mpm, E->sedf, mb.handlers,
+                                                E->bc_tmp, s);
+        if (st != PXB_OK) return st;
+    }
+    return PXB_OK;
+}
+
+int pxb_re_ens_autotune(pxb_re_ens* E, void* stream, int32_t* band_rows) {
+    if (!E) return fail(PXB_ERR_ARG, "null ensemble");
+    cudaStream_t s = (cudaStream_t)stream;
+    return E->dtype == PXB_F64 ? ens_autotune_impl<double>(E, s, band_rows) : ens_autotune_impl<float>(E, s, band_rows);
+}
+
+int pxb_re_ens_run(pxb_re_ens* E, int32_t nsteps, int32_t scheme, double cfl, void* dt_log, void* stream) {
+    if (!E) return fail(PXB_ERR_ARG, "null ensemble");
+    if (nsteps < 0) return fail(PXB_ERR_ARG, "nsteps < 0");
+    if (scheme != PXB_FE && scheme != PXB_SSPRK2) return fail(PXB_ERR_ARG, "scheme must be PXB_FE or PXB_SSPRK2");
+    if (nsteps == 0) return PXB_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    return E->dtype == PXB_F64 ? ens_run_impl<double>(E, nsteps, scheme, cfl, dt_log, s)
+                               : ens_run_impl<float>(E, nsteps, scheme, cfl, dt_log, s);
+}
+
+int pxb_re_ens_check(pxb_re_ens* E, void* stream, int32_t* first_bad) {
+    if (!E) return fail(PXB_ERR_ARG, "null ensemble");
+    cudaStream_t s = (cudaStream_t)stream;
+    std::vector<pxb::CflScratch> h((size_t)E->nm);
+    PXB_CUDA(cudaMemcpyAsync(h.data(), E->scr, sizeof(pxb::CflScratch) * E->nm, cudaMemcpyDeviceToHost, s));
+    PXB_CUDA(cudaStreamSynchronize(s));
+    int bad = -1, code = 0;
+    for (int k = 0; k < E->nm; ++k)
+        if (h[(size_t)k].err != 0 && bad < 0) {
+            bad = k;
+            code = h[(size_t)k].err;
+        }
+    if (first_bad) *first_bad = bad;
+    if (bad < 0) return PXB_OK;
+    PXB_CUDA(cudaMemset2DAsync(&E->scr[0].err, sizeof(pxb::CflScratch), 0, sizeof(int), E->nm, s));
+    PXB_CUDA(cudaStreamSynchronize(s));
+    return fail(PXB_ERR_NONFINITE, "member " + std::to_string(bad) +
+                                       ((code & 2) ? ": non-finite time step" : ": non-finite value in the updated state"));
 }
 
 int pxb_roe_plan_create(const pxb_roe_config* cfg, pxb_roe_plan** out) {

@@ -78,6 +78,59 @@ cudaError_t launch_bc(const BcArgs<T>& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+template <class T, bool MPM, bool HM, bool AVG>
+static cudaError_t ens_variant(const EnsStageArgs<T>& a, int grid, cudaStream_t s) {
+    ens_stage_kernel<T, MPM, HM, AVG><<<grid, 128, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t launch_ens_stage(const EnsStageArgs<T>& a, bool mpm, bool hm, bool avg, int grid, cudaStream_t s) {
+    const int key = (mpm ? 4 : 0) | (hm ? 2 : 0) | (avg ? 1 : 0);
+    switch (key) {
+        case 0: return ens_variant<T, false, false, false>(a, grid, s);
+        case 1: return ens_variant<T, false, false, true>(a, grid, s);
+        case 2: return ens_variant<T, false, true, false>(a, grid, s);
+        case 3: return ens_variant<T, false, true, true>(a, grid, s);
+        case 4: return ens_variant<T, true, false, false>(a, grid, s);
+        case 5: return ens_variant<T, true, false, true>(a, grid, s);
+        case 6: return ens_variant<T, true, true, false>(a, grid, s);
+        default: return ens_variant<T, true, true, true>(a, grid, s);
+    }
+}
+
+template <class T, bool MPM, bool HM, bool AVG>
+static int ens_occ() {
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ens_stage_kernel<T, MPM, HM, AVG>, 128, 0);
+    return n;
+}
+
+template <class T>
+int ens_stage_blocks_per_sm(bool mpm, bool hm, bool avg) {
+    const int key = (mpm ? 4 : 0) | (hm ? 2 : 0) | (avg ? 1 : 0);
+    switch (key) {
+        case 0: return ens_occ<T, false, false, false>();
+        case 1: return ens_occ<T, false, false, true>();
+        case 2: return ens_occ<T, false, true, false>();
+        case 3: return ens_occ<T, false, true, true>();
+        case 4: return ens_occ<T, true, false, false>();
+        case 5: return ens_occ<T, true, false, true>();
+        case 6: return ens_occ<T, true, true, false>();
+        default: return ens_occ<T, true, true, true>();
+    }
+}
+
+template <class T>
+cudaError_t launch_ens_cfl(const EnsCflArgs<T>& a, bool hm, int grid, cudaStream_t s) {
+    if (hm) ens_cfl_kernel<T, true><<<grid, 256, 0, s>>>(a);
+    else ens_cfl_kernel<T, false><<<grid, 256, 0, s>>>(a);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    ens_cfl_finalize_kernel<T><<<(a.nmembers + 127) / 128, 128, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
 template <class T>
 cudaError_t launch_re_general(const GenArgs<T>& a, int phase, cudaStream_t s) {
     dim3 b(32, 8), g((a.nx + 31) / 32, (a.ny + 7) / 8);
@@ -119,6 +172,9 @@ cudaError_t launch_roe_cfl(const CflArgs<T>& a, int grid, cudaStream_t s) {
     template cudaError_t launch_re_init<T>(const InitArgs<T>&, cudaStream_t);                           \
     template cudaError_t launch_bc<T>(const BcArgs<T>&, cudaStream_t);                                  \
     template cudaError_t launch_re_general<T>(const GenArgs<T>&, int, cudaStream_t);                    \
+    template cudaError_t launch_ens_stage<T>(const EnsStageArgs<T>&, bool, bool, bool, int, cudaStream_t); \
+    template int ens_stage_blocks_per_sm<T>(bool, bool, bool);                                          \
+    template cudaError_t launch_ens_cfl<T>(const EnsCflArgs<T>&, bool, int, cudaStream_t);              \
     template cudaError_t launch_set_time<T>(CflScratch*, double, cudaStream_t);                         \
     template cudaError_t launch_roe_stage<T>(const RoeArgs<T>&, bool, cudaStream_t);                    \
     template cudaError_t launch_roe_cfl<T>(const CflArgs<T>&, int, cudaStream_t);

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "ens.cuh"
 #include "init_bc.cuh"
 #include "re_cfl.cuh"
 #include "re_general.cuh"
@@ -33,6 +34,12 @@ template <class T>
 cudaError_t launch_re_general(const GenArgs<T>& a, int phase, cudaStream_t s);
 template <class T>
 cudaError_t launch_set_time(CflScratch* scr, double t0, cudaStream_t s);
+template <class T>
+cudaError_t launch_ens_stage(const EnsStageArgs<T>& a, bool mpm, bool has_mask, bool avg, int grid, cudaStream_t s);
+template <class T>
+int ens_stage_blocks_per_sm(bool mpm, bool has_mask, bool avg);
+template <class T>
+cudaError_t launch_ens_cfl(const EnsCflArgs<T>& a, bool has_mask, int grid, cudaStream_t s);
 template <class T>
 cudaError_t launch_roe_stage(const RoeArgs<T>& a, bool avg, cudaStream_t s);
 template <class T>

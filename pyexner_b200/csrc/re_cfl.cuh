@@ -46,16 +46,14 @@ struct CflArgs {
     int band_rows, nstrips, nbands;
 };
 
+// Largest face-speed bit pattern seen by this lane over one work item (a 32-column strip
+// of one band) folded into `best`; shared by the single-grid and the ensemble kernels.
 template <class T, bool HAS_MASK>
-__global__ void __launch_bounds__(256) re_cfl_kernel(const CflArgs<T> a) {
+__device__ __forceinline__ void re_cfl_item(const CflArgs<T>& a, const int item, unsigned long long& best) {
     const int lane = threadIdx.x & 31;
-    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
     const int ny = a.ny, nx = a.nx;
     const T DRY = T(DRY_TOL);
-    unsigned long long best = 0ull;
-    const int nitems = a.nstrips * a.nbands;
-    for (int item = wid; item < nitems; item += nw) {
+    {
         const int band = item / a.nstrips;
         const int strip = item - band * a.nstrips;
         const int c = strip * 31 + lane;
@@ -102,6 +100,16 @@ __global__ void __launch_bounds__(256) re_cfl_kernel(const CflArgs<T> a) {
             mprev = m;
         }
     }
+}
+
+template <class T, bool HAS_MASK>
+__global__ void __launch_bounds__(256) re_cfl_kernel(const CflArgs<T> a) {
+    const int lane = threadIdx.x & 31;
+    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    unsigned long long best = 0ull;
+    const int nitems = a.nstrips * a.nbands;
+    for (int item = wid; item < nitems; item += nw) re_cfl_item<T, HAS_MASK>(a, item, best);
     // warp max, one atomic per warp
     for (int o = 16; o > 0; o >>= 1) {
         const unsigned long long other = __shfl_xor_sync(FULL, best, o);

@@ -78,21 +78,18 @@ __device__ __forceinline__ ECell<T> shfl_down_ecell(const ECell<T>& p) {
     return q;
 }
 
+// One work item (a strip of one band) of a stage; the single-grid kernel and the
+// ensemble kernel (ens_stage.cuh) both loop over items and call this.
 template <class T, bool MPM, bool HAS_MASK, bool AVG>
-__global__ void __launch_bounds__(128, PXB_STAGE_MIN_BLOCKS) re_stage_kernel(const REStageArgs<T> a) {
+__device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int item, bool& bad) {
     const int lane = threadIdx.x & 31;
-    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
     const int ny = a.ny, nx = a.nx;
     const unsigned upitch = (unsigned)a.pitch;  // planes are < 2^31 elements (checked at plan creation)
     const T dt = *a.dt;
     const T dx = a.dx;
     const T dtdx = dt / dx;  // float path only
     const T DRY = T(DRY_TOL);
-    const int nitems = a.nstrips * a.nbands;
-    bool bad = false;
-
-    for (int item = wid; item < nitems; item += nw) {
+    {
         const int band = item / a.nstrips;
         const int strip = item - band * a.nstrips;
         const int c = strip * PXB_STRIP_OUT - PXB_HALO + lane;
@@ -379,6 +376,15 @@ __global__ void __launch_bounds__(128, PXB_STAGE_MIN_BLOCKS) re_stage_kernel(con
         for (; r < steady1; ++r) iterate(r, std::true_type{});
         for (; r < L1 + 5; ++r) iterate(r, std::false_type{});
     }
+}
+
+template <class T, bool MPM, bool HAS_MASK, bool AVG>
+__global__ void __launch_bounds__(128, PXB_STAGE_MIN_BLOCKS) re_stage_kernel(const REStageArgs<T> a) {
+    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    const int nitems = a.nstrips * a.nbands;
+    bool bad = false;
+    for (int item = wid; item < nitems; item += nw) re_stage_item<T, MPM, HAS_MASK, AVG>(a, item, bad);
     if (bad) atomicOr(a.err, 1);
 }
 
