@@ -17,7 +17,10 @@ Reported:
   fp64       the same loop in float64 (the plain FP64 GPU path) and its speed ratio;
   accuracy   rel-L1 of h and z+z_b, float32 vs float64 after the accuracy run;
   cpu_baseline  the float64 C/OpenMP oracle (all host threads) on a 512 x 512 sample of
-             the same generator, about 10 s of CPU work.
+             the same generator, about 10 s of CPU work;
+  ensemble   the ragged ensemble workload (64 Roe-Exner dam breaks, sides U{128..1024},
+             own beds, step heights and dts; float32; 1000 SSPRK2 steps): autotuned band
+             height, cell-updates/s over all members (state ~1.1 GB, larger than L2).
 
 ``--impl reference`` times the reference algorithm on the CPU instead (the float64
 C/OpenMP restatement of PyExner's JAX step, oracle/c; JAX itself is not installed on
@@ -302,6 +305,46 @@ def accuracy_run(n, steps):
             "hu_rel_l1": l1(a["hu"][s], b["hu"][s])}
 
 
+def ensemble_run(count, steps, seed=0):
+    """The ragged ensemble: ``count`` dam breaks of random sizes advanced together, one
+    launch per phase for all members, every member with its own dt."""
+    import torch
+
+    from pyexner_b200 import BoundaryManager, RoeExnerState
+    from pyexner_b200.boundaries import index_coords
+    from pyexner_b200.cases import ensemble_case, seds_matrix
+    from pyexner_b200.ensemble import Ensemble
+
+    members, erosion = ensemble_case(count, seed)
+    seds = seds_matrix(erosion)
+    mbs = []
+    for m in members:
+        ny, nx = m["shape"]
+        X, Y = index_coords(ny, nx)
+        mbs.append(dict(state=RoeExnerState.from_numpy(m["arrs"], seds, torch.float32),
+                        boundaries=BoundaryManager(m["params"], X, Y), dx=m["dx"]))
+    ens = Ensemble(mbs, erosion)
+    ens.init()
+    rows = ens.autotune()
+    ens.run(3, "SSPRK2", 0.5)  # warm-up: captures the step graph
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.current_stream()
+    e0.record(stream)
+    dts = ens.run(steps, "SSPRK2", 0.5)
+    e1.record(stream)
+    e1.synchronize()
+    sec = e0.elapsed_time(e1) / 1e3
+    ens.check()
+    cells = ens.cells()
+    d = dts.double()
+    return {"workload": f"roe_exner_ragged_ensemble_{count}_dambreaks_128-1024_mpm_ssprk2_f32",
+            "members": count, "cells": cells, "steps": steps, "value": cells * steps / sec, "unit": UNIT,
+            "ms_per_step": 1e3 * sec / steps, "band_rows": rows, "launches_per_step": 4,
+            "dt_range": [float(d.min()), float(d.max())], "l2": "state ~1.1 GB, larger than L2"}
+
+
 def _oracle_case(n):
     from oracle import boundaries as OB
     from oracle import c_oracle as CO
@@ -388,6 +431,8 @@ def main():
     ap.add_argument("--n-big", type=int, default=8192, help="side of the bandwidth case (0 to skip)")
     ap.add_argument("--big-steps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ensemble-members", type=int, default=64, help="ragged ensemble size (0 to skip)")
+    ap.add_argument("--ensemble-steps", type=int, default=1000)
     ap.add_argument("--profile", action="store_true",
                     help="short fixed sequence for ncu: build the case, run --warmup SSPRK2 steps, exit")
     ap.add_argument("--dtype", default="f32", choices=["f32", "f64"])
@@ -466,6 +511,7 @@ def main():
     e2e_sec, h2d, d2h = e2e_run(n, torch.float32, args.steps, args.warmup)
     e2e_val = ncell * args.steps / e2e_sec
     acc = accuracy_run(n, args.accuracy_steps) if args.accuracy_steps > 0 else None
+    ens = ensemble_run(args.ensemble_members, args.ensemble_steps) if args.ensemble_members > 0 else None
     if rank != 0:
         if world > 1:
             dist.barrier()
@@ -488,6 +534,7 @@ def main():
                      "ms": {k: 1e3 * v for k, v in kt.items()}},
         "fp64": {"value": value64, "unit": UNIT, "fp32_over_fp64": value / world / value64},
         "bandwidth_case": big,
+        "ensemble": ens,
         "accuracy": acc,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,

@@ -153,6 +153,13 @@ int pxb_re_init(pxb_re_plan* plan, const pxb_re_fields* f, void* stream);
 /* The stage path the plan resolved to: PXB_PATH_FUSED or PXB_PATH_GENERAL. */
 int pxb_re_plan_path(const pxb_re_plan* plan);
 
+/* Autotuner of the fused stage kernel's band height (no counterpart in the reference):
+ * times a set of heights on stage a -> b (plain and SSPRK2-averaged with a; `a` is not
+ * written, `b` is scratch) and keeps the fastest for the plan; *band_rows (may be NULL)
+ * receives it, 0 on the general path.  Synchronises `stream`. */
+int pxb_re_autotune(pxb_re_plan* plan, const pxb_re_fields* a, const pxb_re_fields* b, void* stream,
+                    int32_t* band_rows);
+
 /* compute_dt_roeexner (roe_exner_solver.py:118-122): dt = max(cfl * min_faces dt_face, 1e-6)
  * written to dt_dev (one element of the plan dtype, device memory). */
 int pxb_re_cfl(pxb_re_plan* plan, const pxb_re_fields* f, double cfl, void* dt_dev, void* stream);

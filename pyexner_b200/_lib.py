@@ -125,6 +125,7 @@ SIGNATURES = {
     "pxb_re_plan_destroy": [c_void_p],
     "pxb_re_init": [c_void_p, POINTER(REFields), c_void_p],
     "pxb_re_plan_path": [c_void_p],
+    "pxb_re_autotune": [c_void_p, POINTER(REFields), POINTER(REFields), c_void_p, POINTER(c_int32)],
     "pxb_re_cfl": [c_void_p, POINTER(REFields), c_double, c_void_p, c_void_p],
     "pxb_re_stage": [c_void_p, POINTER(REFields), POINTER(REFields), POINTER(REFields), c_void_p, c_double,
                      c_void_p],

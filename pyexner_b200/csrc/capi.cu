@@ -13,6 +13,7 @@
 //   * capture the fixed-step integrator loops into CUDA graphs and replay them.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -291,8 +292,11 @@ Geometry stage_geometry(int ny, int nx, int resident_warps, int want_rows) {
     g.nstrips = std::max(1, (nx - 3 + PXB_STRIP_OUT - 1) / PXB_STRIP_OUT);
     int rows = want_rows;
     if (rows <= 0) {
+        // enough bands to give every resident warp an item, but no band taller than 128
+        // rows: on large grids several waves of shorter bands keep the concurrently active
+        // items close together in memory (halo rows and columns shared through L2)
         const int target_bands = std::max(1, resident_warps / g.nstrips);
-        rows = std::max(8, (ny - 1 + target_bands - 1) / target_bands);
+        rows = std::max(8, std::min(128, (ny - 1 + target_bands - 1) / target_bands));
     }
     g.band_rows = rows;
     g.nbands = std::max(1, (ny - 1 + rows - 1) / rows);
@@ -836,6 +840,66 @@ int re_init_impl(pxb_re_plan* P, const pxb_re_fields* f, cudaStream_t s) {
                           P->c.bc_tmp, s);
 }
 
+// Band heights of the fused stage kernel timed on this state (stage a -> b, plain and
+// averaged with a; a is not written); the fastest is kept for every variant.
+template <class T>
+int re_autotune_impl(pxb_re_plan* P, const pxb_re_fields* A, const pxb_re_fields* B, cudaStream_t s, int32_t* out) {
+    const bool f64 = P->c.dtype == PXB_F64;
+    auto set_rows = [&](int rows) {
+        for (int v = 0; v < 8; ++v) {
+            const bool mpm = v & 4, hm = v & 2, avg = v & 1;
+            const int bps = f64 ? pxb::re_stage_blocks_per_sm<double>(mpm, hm, avg)
+                                : pxb::re_stage_blocks_per_sm<float>(mpm, hm, avg);
+            P->stage[v] = stage_geometry(P->c.ny, P->c.nx, std::max(1, bps) * 4 * P->c.sm_count, rows);
+        }
+    };
+    set_rows(0);
+    const int r0 = P->stage[(P->mpm ? 4 : 0) | (P->nodata ? 2 : 0)].band_rows;
+    std::vector<int> cand = {r0, 2 * r0, 3 * r0, 4 * r0, 8, 16, 24, 32, 48, 64, 96, 128, 192, 256};
+    std::vector<int> uniq;
+    for (int c : cand)
+        if (c >= 8 && c <= std::max(8, P->c.ny) && std::find(uniq.begin(), uniq.end(), c) == uniq.end())
+            uniq.push_back(c);
+    pxb_re_fields Bs = *B;
+    Bs.z = A->z;
+    Bs.n_b = A->n_b;
+    int st = re_cfl_impl<T>(P, A, 0.5, P->c.dt_dev, nullptr, s);  // a dt for the timed stages
+    if (st != PXB_OK) return st;
+    cudaEvent_t e0, e1;
+    PXB_CUDA(cudaEventCreate(&e0));
+    PXB_CUDA(cudaEventCreate(&e1));
+    float best_ms = 1e30f;
+    int best = r0;
+    for (int rows : uniq) {
+        set_rows(rows);
+        float ms = 1e30f;
+        for (int rep = 0; rep < 4 && st == PXB_OK; ++rep) {  // the first repetition warms up
+            cudaEventRecord(e0, s);
+            st = re_stage_impl<T>(P, A, &Bs, nullptr, P->c.dt_dev, s);
+            if (st == PXB_OK) st = re_stage_impl<T>(P, A, &Bs, A, P->c.dt_dev, s);
+            cudaEventRecord(e1, s);
+            cudaEventSynchronize(e1);
+            float t = 0;
+            cudaEventElapsedTime(&t, e0, e1);
+            if (rep > 0) ms = std::min(ms, t);
+        }
+        if (st != PXB_OK) break;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = rows;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != PXB_OK) return st;
+    P->want_rows = best;
+    set_rows(best);
+    for (auto& g : P->c.graphs) cudaGraphExecDestroy(g.exec);  // captured with the old geometry
+    P->c.graphs.clear();
+    if (out) *out = best;
+    return PXB_OK;
+}
+
 // One stage on the plan's path; the general path reads the time from *tptr or tval.
 int re_stage_any(pxb_re_plan* P, const pxb_re_fields* in, const pxb_re_fields* out, const pxb_re_fields* avg,
                  const void* dt, const double* tptr, double tval, cudaStream_t s) {
@@ -1276,6 +1340,23 @@ int pxb_re_plan_destroy(pxb_re_plan* plan) {
 }
 
 int pxb_re_plan_path(const pxb_re_plan* plan) { return plan ? plan->path : 0; }
+
+int pxb_re_autotune(pxb_re_plan* P, const pxb_re_fields* a, const pxb_re_fields* b, void* stream, int32_t* band_rows) {
+    if (!P) return fail(PXB_ERR_ARG, "null plan");
+    int st = check_fields(a, true);
+    if (st) return st;
+    st = check_fields(b, true);
+    if (st) return st;
+    if (!a->z || !a->n_b) return fail(PXB_ERR_ARG, "z and n_b must be set");
+    if (a->h == b->h || a->z_b == b->z_b) return fail(PXB_ERR_ARG, "b must not alias a");
+    if (P->path != PXB_PATH_FUSED) {  // the general path has no band geometry
+        if (band_rows) *band_rows = 0;
+        return PXB_OK;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    return P->c.dtype == PXB_F64 ? re_autotune_impl<double>(P, a, b, s, band_rows)
+                                 : re_autotune_impl<float>(P, a, b, s, band_rows);
+}
 
 int pxb_re_init(pxb_re_plan* P, const pxb_re_fields* f, void* stream) {
     if (!P) return fail(PXB_ERR_ARG, "null plan");

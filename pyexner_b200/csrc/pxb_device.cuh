@@ -339,9 +339,9 @@ __device__ __forceinline__ T mpm_grass(T h, T hu, T hv, bool nodata, const SedTa
         float rcb = f_ex2(-0.33333333333f * f_lg2(hc));  // h^(-1/3)
         rcb = rcb * (4.f - hc * rcb * rcb * rcb) * (1.f / 3.f);
         float G = 0.f;
-#pragma unroll
-        for (int k = 0; k < PXB_MAX_SED; ++k) {
-            if (k < S.n) {
+#pragma unroll 1
+        for (int k = 0; k < S.n; ++k) {
+            {
                 const float th = fmaxf(S.k_theta[k] * vel2 * rcb, 0.f);
                 const float dth = th - S.s[k].thc;
                 // below the Shields threshold G is 0: skip the block when no lane is above it
@@ -430,7 +430,10 @@ __device__ __forceinline__ void cubic_extremes(T ut, T at, T ct, T& lmin, T& lma
         const float d = -(ct * ct) * at * ut;
         const float p = (-3.f * c - b * b) * (1.f / 3.f);
         const float q = (2.f * b * b * b + 9.f * b * c + 27.f * d) * (-1.f / 27.f);
-        const float xr = (3.f * q) / (2.f * p) * sqrtf(-3.f / p);
+        // (3q / 2p) sqrt(-3/p); p < 0 for three real roots, otherwise this is NaN and the
+        // float64 solve below takes over
+        const float rp = f_rcp(p);
+        const float xr = 1.5f * q * rp * f_sqrt(-3.f * rp);
         if (fabsf(xr) > 0.999f || xr != xr) {
             double dl, du;
             cubic_extremes<double>(double(ut), double(at), double(ct), dl, du);
@@ -439,10 +442,11 @@ __device__ __forceinline__ void cubic_extremes(T ut, T at, T ct, T& lmin, T& lma
             return;
         }
         const float th = acosf(xr);
-        const float sq = 2.f * sqrtf(-p * (1.f / 3.f));
+        const float sq = 2.f * f_sqrt(-p * (1.f / 3.f));
         const float shift = b * (1.f / 3.f);
+        // th / 3 is in [0, pi/3]: the hardware sine / cosine are within 2^-21 absolute there
         float sn, cs;
-        sincosf(th * (1.f / 3.f), &sn, &cs);
+        __sincosf(th * (1.f / 3.f), &sn, &cs);
         lmax = sq * cs + shift;
         // cos((th + 2 pi)/3) = -cos(th/3)/2 - sqrt(3)/2 sin(th/3)
         lmin = sq * (-0.5f * cs - 0.86602540378f * sn) + shift;

@@ -95,6 +95,17 @@ def run_steps(state, mask, solver_config, scheme, n_steps, cfl, scratch=None, lo
     return dts[:n_steps] if dts is not None else None
 
 
+def autotune(state, mask, solver_config, scratch=None):
+    """Time the fused stage kernel's band heights on ``state`` (left unchanged) and keep
+    the fastest in the plan; returns it (0 on the general path)."""
+    b = scratch if scratch is not None else scratch_like(state)
+    plan = _re_plan(state, mask, solver_config)
+    out = ctypes.c_int32(0)
+    _lib.call("pxb_re_autotune", plan.handle, ctypes.byref(state.c_fields()), ctypes.byref(b.c_fields()), _stream(),
+              ctypes.byref(out))
+    return int(out.value)
+
+
 def check_state(state, mask, solver_config):
     """Raise if a kernel flagged a non-finite dt or state value since the last check."""
     if isinstance(state, RoeExnerState):
