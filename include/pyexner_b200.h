@@ -273,6 +273,20 @@ int pxb_re_cfl_noalloc(int32_t ny, int32_t nx, int64_t pitch, int32_t dtype, dou
                        const void* h, const void* hu, const void* hv, const void* G, const uint8_t* nodata,
                        void* dt_dev, void* stream);
 
+/* --- boundary set-up on the device ------------------------------------------------- */
+/* The polygon labelling of BoundaryManager (boundary_registry.py:19-59) and the
+ * raster-order cell lists its index maps start from (:61-82), for large grids.  Cell
+ * centres are the outer product of xc[nx] (x of each column) and yc[ny] (y of each row),
+ * host arrays; verts: host array npoly x nverts x 2 (x, y), each polygon zero-padded to
+ * nverts as the reference pads it.  counts[npoly] (host) receives the number of cells
+ * inside each polygon (even-odd rule, 1e-8 tolerance on the crossing abscissa); when
+ * `cells` is not NULL it receives, polygon after polygon, the flat indices row*nx + col
+ * of those cells in raster order (capacity cells_cap; PXB_ERR_ARG if too small, counts
+ * still filled).  Allocates device scratch for the call; synchronises `stream`. */
+int pxb_label_polygons(int32_t ny, int32_t nx, const double* xc, const double* yc, const double* verts,
+                       int32_t npoly, int32_t nverts, int64_t* counts, int64_t* cells, int64_t cells_cap,
+                       void* stream);
+
 /* --- misc ------------------------------------------------------------------------- */
 const char* pxb_last_error(void);
 int pxb_version(void);

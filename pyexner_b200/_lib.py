@@ -146,6 +146,8 @@ SIGNATURES = {
     "pxb_re_ens_check": [c_void_p, c_void_p, POINTER(c_int32)],
     "pxb_re_cfl_noalloc": [c_int32, c_int32, c_int64, c_int32, c_double, c_double, c_void_p, c_void_p, c_void_p,
                            c_void_p, c_void_p, c_void_p, c_void_p],
+    "pxb_label_polygons": [c_int32, c_int32, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p, c_void_p,
+                           c_int64, c_void_p],
     "pxb_version": [],
 }
 

@@ -43,19 +43,58 @@ def label_masks(X, Y, polygons):
 
 def index_maps(mask, normal):
     """(boundary cells, donor cells) as (rows, cols) pairs (boundary_registry.py:61-82)."""
+    b = np.argwhere(mask)
+    return donor_maps((b[:, 0], b[:, 1]), normal, mask.shape)
+
+
+def donor_maps(cells, normal, shape):
+    """Donors of raster-ordered boundary cells: one step against the normal,
+    (row + round(ny), col - round(nx)), clipped to the array (boundary_registry.py:61-82)."""
     dx = -int(np.round(normal[0]))
     dy = int(np.round(normal[1]))
-    b = np.argwhere(mask)
-    i = b + np.array([dy, dx])
-    ny, nx = mask.shape
-    i = np.clip(i, 0, np.array([ny - 1, nx - 1]))
-    return (b[:, 0], b[:, 1]), (i[:, 0], i[:, 1])
+    by, bx = cells
+    ny, nx = shape
+    return (by, bx), (np.clip(by + dy, 0, ny - 1), np.clip(bx + dx, 0, nx - 1))
+
+
+def label_cells_device(X, Y, polygons):
+    """Raster-ordered (rows, cols) of the cells inside each polygon, labelled on the GPU
+    (``pxb_label_polygons``) with the host test's arithmetic.  X, Y must be a meshgrid
+    (X constant down columns, Y constant along rows)."""
+    X = np.asarray(X, dtype=np.float64)
+    Y = np.asarray(Y, dtype=np.float64)
+    ny, nx = X.shape
+    xc = np.ascontiguousarray(X[0, :])
+    yc = np.ascontiguousarray(Y[:, 0])
+    if not (np.array_equal(X, np.broadcast_to(xc, X.shape)) and np.array_equal(Y, np.broadcast_to(yc[:, None], Y.shape))):
+        raise ValueError("device labelling needs meshgrid coordinates")
+    nv = max(len(p) for p in polygons)
+    verts = np.zeros((len(polygons), nv, 2))
+    for k, p in enumerate(polygons):
+        p = np.asarray(p, dtype=np.float64)
+        verts[k, : p.shape[0]] = p
+    verts = np.ascontiguousarray(verts)
+    counts = np.zeros(len(polygons), dtype=np.int64)
+    args = (ny, nx, xc.ctypes.data, yc.ctypes.data, verts.ctypes.data, len(polygons), nv, counts.ctypes.data)
+    _lib.call("pxb_label_polygons", *args, None, 0, None)
+    cells = np.empty(max(1, int(counts.sum())), dtype=np.int64)
+    _lib.call("pxb_label_polygons", *args, cells.ctypes.data, int(cells.size), None)
+    out, o = [], 0
+    for n in counts:
+        idx = cells[o:o + n]
+        out.append((idx // nx, idx % nx))
+        o += n
+    return out
 
 
 class BoundaryManager:
-    """Boundary handlers of one run, in YAML order."""
+    """Boundary handlers of one run, in YAML order.
 
-    def __init__(self, params, X, Y):
+    ``setup``: "host" labels the cells with NumPy, "device" on the GPU
+    (``pxb_label_polygons``, for large grids), "auto" picks the device above 4M cells
+    when a GPU is present.  Both give the same cells."""
+
+    def __init__(self, params, X, Y, setup="auto"):
         self.flux_scheme = params["flux_scheme"]
         self.boundary_specs = params.get("boundaries") or {}
         self.names = list(self.boundary_specs)
@@ -66,9 +105,25 @@ class BoundaryManager:
         if not self.names:
             self.boundary_mask = np.zeros(self.shape, bool)
             return
-        masks = label_masks(X, Y, [self.boundary_specs[k]["polygon"] for k in self.names])
-        self.boundary_mask = np.any(np.stack(masks), axis=0)
-        for name, m in zip(self.names, masks):
+        polys = [self.boundary_specs[k]["polygon"] for k in self.names]
+        if setup == "auto":
+            setup = "host"
+            if X.size > (1 << 22):
+                import torch
+
+                if torch.cuda.is_available():
+                    setup = "device"
+        if setup == "device":
+            cell_lists = label_cells_device(X, Y, polys)
+        else:
+            cell_lists = []
+            for m in label_masks(X, Y, polys):
+                b = np.argwhere(m)
+                cell_lists.append((b[:, 0], b[:, 1]))
+        self.boundary_mask = np.zeros(self.shape, bool)
+        for by, bx in cell_lists:
+            self.boundary_mask[by, bx] = True
+        for name, cl in zip(self.names, cell_lists):
             spec = self.boundary_specs[name]
             kind = self.flux_scheme + " " + spec["type"]
             if kind not in _lib.BC_KINDS:
@@ -78,16 +133,15 @@ class BoundaryManager:
             normal = [float(v) for v in spec["normal"]]
             if kind == "Roe Exner ZeroMomentum":
                 # mask handler (roeexner_zeromomentum.py:16-31): every mask cell is its own donor
-                b = np.argwhere(m)
-                (by, bx), (iy, ix) = (b[:, 0], b[:, 1]), (b[:, 0], b[:, 1])
+                (by, bx), (iy, ix) = cl, cl
             else:
-                (by, bx), (iy, ix) = index_maps(m, normal)
+                (by, bx), (iy, ix) = donor_maps(cl, normal, self.shape)
             hu_c = hv_c = 0.0
             if kind == "Roe Exner ConstantInflux":
                 # float32 values as parsed by boundary_registry.py:107-110, product in float32
                 hu_c = float(np.float32(vals[0]) * np.float32(vals[1]))
                 hv_c = float(np.float32(vals[0]) * np.float32(vals[2]))
-            self.handlers.append(dict(name=name, kind=kind, mask=m, normal=normal, values=vals,
+            self.handlers.append(dict(name=name, kind=kind, normal=normal, values=vals,
                                       cells=(by, bx), donors=(iy, ix), hu_const=hu_c, hv_const=hv_c))
 
     def c_array(self, pitch):

@@ -2,9 +2,10 @@
 
     python -m pyexner_b200.build
 
-Three translation units: the float32 kernels, the float64 kernels (with
-``--fmad=false`` so every product and sum rounds on its own, as in the reference's
-float64 arithmetic) and the C ABI.  Objects go to ``pyexner_b200/_build``.
+Translation units: the float32 kernels, the float64 kernels and the set-up kernels
+(both with ``--fmad=false`` so every product and sum rounds on its own, as in the
+reference's float64 arithmetic), the C ABI and the allocation-free time step.  Objects
+go to ``pyexner_b200/_build``.
 """
 from __future__ import annotations
 
@@ -24,6 +25,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 UNITS = [
     ("kernels_f32.cu", []),
     ("kernels_f64.cu", ["-fmad=false"]),
+    ("setup_f64.cu", ["-fmad=false"]),
     ("capi.cu", []),
     ("noalloc.cu", []),
 ]
@@ -57,7 +59,7 @@ def build(force=False, verbose=False):
         return LIB
     os.makedirs(BUILD, exist_ok=True)
     objs = []
-    knobs = os.environ.get("PXB_NVCC_DEFINES", "").split()  # e.g. "-DPXB_ROW_UNROLL=2" for tuning sweeps
+    knobs = os.environ.get("PXB_NVCC_DEFINES", "").split()  # e.g. "-DPXB_STAGE_MIN_BLOCKS=4" for tuning sweeps
     for src, extra in UNITS:
         obj = os.path.join(BUILD, src.replace(".cu", ".o"))
         cmd = [nvcc(), *ARCH, *COMMON, *extra, *knobs, "-c", os.path.join(CSRC, src), "-o", obj]

@@ -1289,6 +1289,73 @@ int ens_autotune_impl(pxb_re_ens* E, cudaStream_t s, int32_t* out) {
 extern "C" {
 
 const char* pxb_last_error(void) { return g_err.c_str(); }
+
+int pxb_label_polygons(int32_t ny, int32_t nx, const double* xc, const double* yc, const double* verts,
+                       int32_t npoly, int32_t nverts, int64_t* counts, int64_t* cells, int64_t cells_cap,
+                       void* stream) {
+    if (ny < 1 || nx < 1 || npoly < 1 || nverts < 1) return fail(PXB_ERR_ARG, "empty grid or polygon set");
+    if (!xc || !yc || !verts || !counts) return fail(PXB_ERR_ARG, "null coordinate, vertex or count array");
+    if ((long long)npoly * ny * nx >= (1LL << 40)) return fail(PXB_ERR_ARG, "label planes too large");
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t rows = (size_t)npoly * ny;
+    double *dx = nullptr, *dy = nullptr, *dv = nullptr;
+    uint8_t* lab = nullptr;
+    long long *cnt = nullptr, *off = nullptr, *dcells = nullptr;
+    std::vector<long long> hc(rows), ho(rows);
+    int code = PXB_OK;
+    std::string msg;
+    auto ok = [&](cudaError_t e, const char* what) {
+        if (e != cudaSuccess && code == PXB_OK) {
+            code = PXB_ERR_CUDA;
+            msg = std::string(what) + ": " + cudaGetErrorString(e);
+        }
+        return code == PXB_OK;
+    };
+    if (ok(cudaMalloc(&dx, sizeof(double) * nx), "coordinates") && ok(cudaMalloc(&dy, sizeof(double) * ny), "coordinates") &&
+        ok(cudaMalloc(&dv, sizeof(double) * 2 * (size_t)npoly * nverts), "vertices") &&
+        ok(cudaMalloc(&lab, rows * (size_t)nx), "labels") && ok(cudaMalloc(&cnt, sizeof(long long) * rows), "counts") &&
+        ok(cudaMemcpyAsync(dx, xc, sizeof(double) * nx, cudaMemcpyHostToDevice, s), "copy") &&
+        ok(cudaMemcpyAsync(dy, yc, sizeof(double) * ny, cudaMemcpyHostToDevice, s), "copy") &&
+        ok(cudaMemcpyAsync(dv, verts, sizeof(double) * 2 * (size_t)npoly * nverts, cudaMemcpyHostToDevice, s), "copy") &&
+        ok(pxb::launch_label(ny, nx, dx, dy, dv, npoly, nverts, lab, s), "label kernel") &&
+        ok(pxb::launch_label_count(ny, nx, npoly, lab, cnt, s), "count kernel") &&
+        ok(cudaMemcpyAsync(hc.data(), cnt, sizeof(long long) * rows, cudaMemcpyDeviceToHost, s), "copy") &&
+        ok(cudaStreamSynchronize(s), "synchronise")) {
+        long long total = 0;
+        for (int p = 0; p < npoly; ++p) {
+            long long n = 0;
+            for (int r = 0; r < ny; ++r) {
+                ho[(size_t)p * ny + r] = total + n;
+                n += hc[(size_t)p * ny + r];
+            }
+            counts[p] = n;
+            total += n;
+        }
+        if (cells) {
+            if (total > cells_cap) {
+                code = PXB_ERR_ARG;
+                msg = "cells capacity " + std::to_string(cells_cap) + " < " + std::to_string(total) + " labelled cells";
+            } else if (total > 0 &&
+                       ok(cudaMalloc(&off, sizeof(long long) * rows), "offsets") &&
+                       ok(cudaMalloc(&dcells, sizeof(long long) * (size_t)total), "cells") &&
+                       ok(cudaMemcpyAsync(off, ho.data(), sizeof(long long) * rows, cudaMemcpyHostToDevice, s), "copy") &&
+                       ok(pxb::launch_label_fill(ny, nx, npoly, lab, off, dcells, s), "fill kernel") &&
+                       ok(cudaMemcpyAsync(cells, dcells, sizeof(long long) * (size_t)total, cudaMemcpyDeviceToHost, s),
+                          "copy")) {
+                ok(cudaStreamSynchronize(s), "synchronise");
+            }
+        }
+    }
+    cudaStreamSynchronize(s);
+    cudaFree(dx);
+    cudaFree(dy);
+    cudaFree(dv);
+    cudaFree(lab);
+    cudaFree(cnt);
+    cudaFree(off);
+    cudaFree(dcells);
+    return code == PXB_OK ? PXB_OK : fail(code, msg);
+}
 int pxb_version(void) { return 1; }
 
 int pxb_re_plan_create(const pxb_re_config* cfg, pxb_re_plan** out) {

@@ -16,6 +16,13 @@ namespace pxb {
 // Records the message returned by pxb_last_error() on this thread; returns `code`.
 int set_error(int code, const std::string& msg);
 
+// Boundary set-up on the device (setup_f64.cu).
+cudaError_t launch_label(int ny, int nx, const double* xc, const double* yc, const double* verts, int npoly, int nv,
+                         uint8_t* labels, cudaStream_t s);
+cudaError_t launch_label_count(int ny, int nx, int npoly, const uint8_t* labels, long long* counts, cudaStream_t s);
+cudaError_t launch_label_fill(int ny, int nx, int npoly, const uint8_t* labels, const long long* offsets,
+                              long long* cells, cudaStream_t s);
+
 template <class T>
 cudaError_t launch_re_stage(const REStageArgs<T>& a, bool mpm, bool has_mask, bool avg, int grid, cudaStream_t s);
 template <class T>
