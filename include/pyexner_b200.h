@@ -183,6 +183,18 @@ int pxb_re_stage(pxb_re_plan* plan, const pxb_re_fields* in, const pxb_re_fields
 int pxb_re_run(pxb_re_plan* plan, const pxb_re_fields* a, const pxb_re_fields* b, int32_t nsteps,
                int32_t scheme, double cfl, double t0, void* dt_log, void* stream);
 
+/* Tangent-linear model (forward-mode derivative) of pxb_re_init / pxb_re_run, float64
+ * plans only.  No counterpart in the reference's code (JAX would give it with jax.jvp).
+ * The state planes and their tangents (every plane of both structs set) advance together:
+ * values bit for bit as the float64 run, tangents by the chain rule through the step
+ * including the state dependence of dt through the fastest face.  The stage runs the
+ * general path's kernels on dual numbers (any boundary layout); the plan allocates its
+ * dual planes on the first call.  dt_log / dt_dot_log: device float64 arrays of nsteps
+ * values / tangents of dt, or NULL. */
+int pxb_re_jvp_init(pxb_re_plan* plan, const pxb_re_fields* f, const pxb_re_fields* f_dot, void* stream);
+int pxb_re_jvp_run(pxb_re_plan* plan, const pxb_re_fields* a, const pxb_re_fields* a_dot, int32_t nsteps,
+                   int32_t scheme, double cfl, double t0, void* dt_log, void* dt_dot_log, void* stream);
+
 /* Device error word of the plan (non-finite dt or state seen by a kernel): reads it
  * (synchronising `stream`), clears it, returns PXB_OK or PXB_ERR_NONFINITE. */
 int pxb_re_check(pxb_re_plan* plan, void* stream);

@@ -26,6 +26,7 @@ UNITS = [
     ("kernels_f32.cu", []),
     ("kernels_f64.cu", ["-fmad=false"]),
     ("setup_f64.cu", ["-fmad=false"]),
+    ("kernels_dual.cu", ["-fmad=false"]),
     ("capi.cu", []),
     ("noalloc.cu", []),
 ]

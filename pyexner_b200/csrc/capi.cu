@@ -550,6 +550,11 @@ struct pxb_re_plan {
     PlanCommon c;
     int path = PXB_PATH_FUSED;
     void* gen = nullptr;  // general path: 7 scratch planes (h, hu, hv, z_b, G, n, z_b after Exner)
+    // tangent-linear model (float64 plans): dual planes and scratch, allocated on first use
+    void* jvp = nullptr;
+    pxb::DualScratch* dscr = nullptr;
+    void* jvp_tmp = nullptr;
+    pxb::SedTable<pxb::Dual> sedD;
     int mpm = 0;
     const uint8_t* nodata = nullptr;
     Geometry stage[8];  // by (mpm, mask, avg) variant: band geometry from its occupancy
@@ -643,6 +648,26 @@ template <>
 const pxb::SedTable<float>& sed_of<float>(const pxb_re_plan* p) { return p->sedf; }
 template <>
 const pxb::SedTable<double>& sed_of<double>(const pxb_re_plan* p) { return p->sedd; }
+template <>
+const pxb::SedTable<pxb::Dual>& sed_of<pxb::Dual>(const pxb_re_plan* p) { return p->sedD; }
+
+// The float64 sediment table as dual numbers with zero tangents.
+void dual_sed(pxb::SedTable<pxb::Dual>& D, const pxb::SedTable<double>& S) {
+    D.n = S.n;
+    for (int k = 0; k < PXB_MAX_SED; ++k) {
+        D.s[k].np2 = S.s[k].np2;
+        D.s[k].sm1d = S.s[k].sm1d;
+        D.s[k].thc = S.s[k].thc;
+        D.s[k].np3sg = S.s[k].np3sg;
+        D.s[k].sm1 = S.s[k].sm1;
+        D.s[k].frac = S.s[k].frac;
+        D.k_theta[k] = S.k_theta[k];
+        D.k_g1[k] = S.k_g1[k];
+    }
+    D.one_minus_por = S.one_minus_por;
+    D.n_p_mix = S.n_p_mix;
+    D.inv_one_minus_por = S.inv_one_minus_por;
+}
 
 int check_fields(const pxb_re_fields* f, bool need_g) {
     if (!f) return fail(PXB_ERR_ARG, "fields pointer is null");
@@ -777,9 +802,11 @@ int init_fields(int ny, int nx, long long pitch, const pxb_re_fields* f, const u
 // One stage on the general path (re_general.cuh).
 template <class T>
 int re_general_impl(pxb_re_plan* P, const pxb_re_fields* in, const pxb_re_fields* out, const pxb_re_fields* avg,
-                    const void* dt, const double* tptr, double tval, cudaStream_t s) {
+                    const void* dt, const double* tptr, double tval, cudaStream_t s, void* scratch = nullptr,
+                    void* bc_tmp = nullptr) {
     const size_t plane = (size_t)P->c.ny * (size_t)P->c.pitch;
-    T* S = (T*)P->gen;
+    T* S = (T*)(scratch ? scratch : P->gen);
+    void* tmp = bc_tmp ? bc_tmp : P->c.bc_tmp;
     pxb::GenArgs<T> a{};
     a.ny = P->c.ny;
     a.nx = P->c.nx;
@@ -823,12 +850,12 @@ int re_general_impl(pxb_re_plan* P, const pxb_re_fields* in, const pxb_re_fields
     PXB_CUDA(pxb::launch_re_general<T>(a, pxb::GEN_HYDRO, s));
     PXB_CUDA(pxb::launch_re_general<T>(a, pxb::GEN_CORR, s));
     T* const f1[6] = {a.sh, a.shu, a.shv, a.szb, a.sn, a.sG};
-    int st = apply_handlers<T>(P->c, f1, tptr, tval, s);
+    int st = apply_handlers<T>(P->c.handlers, tmp, f1, tptr, tval, s);
     if (st != PXB_OK) return st;
     PXB_CUDA(pxb::launch_re_general<T>(a, pxb::GEN_GRASS, s));
     PXB_CUDA(pxb::launch_re_general<T>(a, pxb::GEN_EXNER, s));
     T* const f2[6] = {a.sh, a.shu, a.shv, a.szb2, a.sn, a.sG};
-    st = apply_handlers<T>(P->c, f2, tptr, tval, s);
+    st = apply_handlers<T>(P->c.handlers, tmp, f2, tptr, tval, s);
     if (st != PXB_OK) return st;
     PXB_CUDA(pxb::launch_re_general<T>(a, pxb::GEN_STORE, s));
     return PXB_OK;
@@ -1283,6 +1310,138 @@ int ens_autotune_impl(pxb_re_ens* E, cudaStream_t s, int32_t* out) {
     return PXB_OK;
 }
 
+// ------------------------------------------------------------------ tangent-linear model
+// Dual planes: state A (h, hu, hv, z, z_b, n, n_b, G), state B (same layout; its z and
+// n_b are A's) and the 7 scratch planes of the general path, plus one dual dt.
+int jvp_buffers(pxb_re_plan* P) {
+    if (P->jvp) return PXB_OK;
+    const size_t plane = (size_t)P->c.ny * (size_t)P->c.pitch;
+    PXB_CUDA(cudaMalloc(&P->jvp, sizeof(pxb::Dual) * (plane * 23 + 1)));
+    PXB_CUDA(cudaMalloc(&P->dscr, sizeof(pxb::DualScratch)));
+    PXB_CUDA(cudaMemset(P->dscr, 0, sizeof(pxb::DualScratch)));
+    int maxcount = 1;
+    for (auto& h : P->c.handlers) maxcount = std::max(maxcount, h.count);
+    PXB_CUDA(cudaMalloc(&P->jvp_tmp, sizeof(pxb::Dual) * 6 * (size_t)maxcount));
+    return PXB_OK;
+}
+
+pxb_re_fields dual_state(pxb_re_plan* P, int which) {
+    const size_t plane = (size_t)P->c.ny * (size_t)P->c.pitch;
+    pxb::Dual* b = (pxb::Dual*)P->jvp + (size_t)which * 8 * plane;
+    pxb_re_fields f{};
+    f.h = b;
+    f.hu = b + plane;
+    f.hv = b + 2 * plane;
+    f.z = b + 3 * plane;
+    f.z_b = b + 4 * plane;
+    f.n = b + 5 * plane;
+    f.n_b = b + 6 * plane;
+    f.G = b + 7 * plane;
+    return f;
+}
+
+void field_slots(const pxb_re_fields* f, void* out[8]) {
+    out[0] = f->h;
+    out[1] = f->hu;
+    out[2] = f->hv;
+    out[3] = f->z;
+    out[4] = f->z_b;
+    out[5] = f->n;
+    out[6] = f->n_b;
+    out[7] = f->G;
+}
+
+int jvp_pack(pxb_re_plan* P, const pxb_re_fields* v, const pxb_re_fields* t, const pxb_re_fields* D, cudaStream_t s) {
+    void *vs[8], *ts[8], *ds[8];
+    field_slots(v, vs);
+    field_slots(t, ts);
+    field_slots(D, ds);
+    for (int k = 0; k < 8; ++k)
+        PXB_CUDA(pxb::launch_dual_pack(P->c.ny, P->c.nx, P->c.pitch, (const double*)vs[k], (const double*)ts[k],
+                                       (pxb::Dual*)ds[k], s));
+    return PXB_OK;
+}
+
+int jvp_unpack(pxb_re_plan* P, const pxb_re_fields* D, const pxb_re_fields* v, const pxb_re_fields* t, cudaStream_t s) {
+    void *vs[8], *ts[8], *ds[8];
+    field_slots(v, vs);
+    field_slots(t, ts);
+    field_slots(D, ds);
+    for (int k = 0; k < 8; ++k)
+        PXB_CUDA(pxb::launch_dual_unpack(P->c.ny, P->c.nx, P->c.pitch, (const pxb::Dual*)ds[k], (double*)vs[k],
+                                         (double*)ts[k], s));
+    return PXB_OK;
+}
+
+int check_tangent_fields(const pxb_re_fields* f, const char* what) {
+    if (!f || !f->h || !f->hu || !f->hv || !f->z || !f->z_b || !f->n || !f->n_b || !f->G)
+        return fail(PXB_ERR_ARG, std::string(what) + ": every plane (h, hu, hv, z, z_b, n, n_b, G) must be set");
+    return PXB_OK;
+}
+
+int jvp_init_impl(pxb_re_plan* P, const pxb_re_fields* f, const pxb_re_fields* fd, cudaStream_t s) {
+    int st = jvp_buffers(P);
+    if (st != PXB_OK) return st;
+    const pxb_re_fields DA = dual_state(P, 0);
+    st = jvp_pack(P, f, fd, &DA, s);
+    if (st == PXB_OK)
+        st = init_fields<pxb::Dual>(P->c.ny, P->c.nx, P->c.pitch, &DA, P->nodata, P->mpm, P->sedD, P->c.handlers,
+                                    P->jvp_tmp, s);
+    if (st == PXB_OK) st = jvp_unpack(P, &DA, f, fd, s);
+    return st;
+}
+
+int jvp_run_impl(pxb_re_plan* P, const pxb_re_fields* a, const pxb_re_fields* ad, int nsteps, int scheme, double cfl,
+                 double t0, double* dt_log, double* dt_dot_log, cudaStream_t s) {
+    int st = jvp_buffers(P);
+    if (st != PXB_OK) return st;
+    const size_t plane = (size_t)P->c.ny * (size_t)P->c.pitch;
+    pxb_re_fields DA = dual_state(P, 0), DB = dual_state(P, 1);
+    DB.z = DA.z;
+    DB.n_b = DA.n_b;
+    void* gscr = (pxb::Dual*)P->jvp + 16 * plane;
+    pxb::Dual* dtd = (pxb::Dual*)P->jvp + 23 * plane;
+    st = jvp_pack(P, a, ad, &DA, s);
+    if (st != PXB_OK) return st;
+    pxb::DualScratch init{};
+    init.t_step = t0;
+    init.t_next = t0;
+    PXB_CUDA(cudaMemcpyAsync(P->dscr, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+    PXB_CUDA(cudaStreamSynchronize(s));  // `init` lives on this stack frame
+    const double* tdev = &P->dscr->t_step;
+    pxb_re_fields* cur = &DA;
+    pxb_re_fields* nxt = &DB;
+    for (int k = 0; k < nsteps && st == PXB_OK; ++k) {
+        pxb::DualCflArgs c{};
+        c.ny = P->c.ny;
+        c.nx = P->c.nx;
+        c.pitch = P->c.pitch;
+        c.h = (const pxb::Dual*)cur->h;
+        c.hu = (const pxb::Dual*)cur->hu;
+        c.hv = (const pxb::Dual*)cur->hv;
+        c.G = (const pxb::Dual*)cur->G;
+        c.nodata = P->nodata;
+        c.dx = P->c.dx;
+        c.cfl = cfl;
+        c.floor_dt = pxb::DT_FLOOR;
+        c.scr = P->dscr;
+        c.dt_out = dtd;
+        c.dt_log = dt_log;
+        c.dt_dot_log = dt_dot_log;
+        c.err = &P->c.scr->err;
+        PXB_CUDA(pxb::launch_dual_cfl(c, s));
+        if (scheme == PXB_SSPRK2) {
+            st = re_general_impl<pxb::Dual>(P, cur, nxt, nullptr, dtd, tdev, 0.0, s, gscr, P->jvp_tmp);
+            if (st == PXB_OK) st = re_general_impl<pxb::Dual>(P, nxt, cur, cur, dtd, tdev, 0.0, s, gscr, P->jvp_tmp);
+        } else {
+            st = re_general_impl<pxb::Dual>(P, cur, nxt, nullptr, dtd, tdev, 0.0, s, gscr, P->jvp_tmp);
+            std::swap(cur, nxt);
+        }
+    }
+    if (st != PXB_OK) return st;
+    return jvp_unpack(P, cur, a, ad, s);
+}
+
 }  // namespace
 
 // ===================================================================== C entry points
@@ -1382,6 +1541,7 @@ int pxb_re_plan_create(const pxb_re_config* cfg, pxb_re_plan** out) {
     if (cfg->mpm) {
         fill_sed(P->sedf, cfg->seds, cfg->nsed);
         fill_sed(P->sedd, cfg->seds, cfg->nsed);
+        dual_sed(P->sedD, P->sedd);
     }
     const bool f64 = cfg->dtype == PXB_F64;
     for (int v = 0; v < 8; ++v) {
@@ -1402,6 +1562,9 @@ int pxb_re_plan_destroy(pxb_re_plan* plan) {
     cudaDeviceSynchronize();
     plan->c.release();
     cudaFree(plan->gen);
+    cudaFree(plan->jvp);
+    cudaFree(plan->dscr);
+    cudaFree(plan->jvp_tmp);
     delete plan;
     return PXB_OK;
 }
@@ -1473,6 +1636,29 @@ int pxb_re_run(pxb_re_plan* P, const pxb_re_fields* a, const pxb_re_fields* b, i
     if (scheme != PXB_FE && scheme != PXB_SSPRK2) return fail(PXB_ERR_ARG, "scheme must be PXB_FE or PXB_SSPRK2");
     if (nsteps == 0) return PXB_OK;
     return re_steps(P, a, b, nsteps, scheme, cfl, t0, dt_log, (cudaStream_t)stream);
+}
+
+int pxb_re_jvp_init(pxb_re_plan* P, const pxb_re_fields* f, const pxb_re_fields* f_dot, void* stream) {
+    if (!P) return fail(PXB_ERR_ARG, "null plan");
+    if (P->c.dtype != PXB_F64) return fail(PXB_ERR_ARG, "the tangent-linear model runs on float64 plans");
+    int st = check_tangent_fields(f, "state");
+    if (st == PXB_OK) st = check_tangent_fields(f_dot, "tangent");
+    if (st != PXB_OK) return st;
+    return jvp_init_impl(P, f, f_dot, (cudaStream_t)stream);
+}
+
+int pxb_re_jvp_run(pxb_re_plan* P, const pxb_re_fields* a, const pxb_re_fields* a_dot, int32_t nsteps, int32_t scheme,
+                   double cfl, double t0, void* dt_log, void* dt_dot_log, void* stream) {
+    if (!P) return fail(PXB_ERR_ARG, "null plan");
+    if (P->c.dtype != PXB_F64) return fail(PXB_ERR_ARG, "the tangent-linear model runs on float64 plans");
+    int st = check_tangent_fields(a, "state");
+    if (st == PXB_OK) st = check_tangent_fields(a_dot, "tangent");
+    if (st != PXB_OK) return st;
+    if (nsteps < 0) return fail(PXB_ERR_ARG, "nsteps < 0");
+    if (scheme != PXB_FE && scheme != PXB_SSPRK2) return fail(PXB_ERR_ARG, "scheme must be PXB_FE or PXB_SSPRK2");
+    if (nsteps == 0) return PXB_OK;
+    return jvp_run_impl(P, a, a_dot, nsteps, scheme, cfl, t0, (double*)dt_log, (double*)dt_dot_log,
+                        (cudaStream_t)stream);
 }
 
 int pxb_re_check(pxb_re_plan* P, void* stream) {

@@ -8,6 +8,7 @@
 #include "re_general.cuh"
 #include "re_stage.cuh"
 #include "roe_plain.cuh"
+#include "dual.cuh"
 
 #include <string>
 
@@ -41,6 +42,12 @@ template <class T>
 cudaError_t launch_re_general(const GenArgs<T>& a, int phase, cudaStream_t s);
 template <class T>
 cudaError_t launch_set_time(CflScratch* scr, double t0, cudaStream_t s);
+
+// Tangent-linear model (kernels_dual.cu).
+cudaError_t launch_dual_cfl(const DualCflArgs& a, cudaStream_t s);
+cudaError_t launch_dual_pack(int ny, int nx, long long pitch, const double* v, const double* t, Dual* out,
+                             cudaStream_t s);
+cudaError_t launch_dual_unpack(int ny, int nx, long long pitch, const Dual* in, double* v, double* t, cudaStream_t s);
 template <class T>
 cudaError_t launch_ens_stage(const EnsStageArgs<T>& a, bool mpm, bool has_mask, bool avg, int grid, cudaStream_t s);
 template <class T>

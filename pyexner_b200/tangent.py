@@ -1,0 +1,111 @@
+"""Tangent-linear model of the float64 Roe-Exner step (forward-mode derivatives).
+
+For a state ``u`` and a direction ``u_dot`` (a second RoeExnerState holding the tangent
+of every plane), ``jvp_run`` advances both through ``n_steps`` integrator steps: the
+values exactly as ``run_steps`` does in float64, the tangents by the chain rule through
+every stage, including the dependence of dt on the state (through the fastest face).
+This is what ``jax.jvp`` of the reference's loop would give; gradients of a scalar
+objective follow one direction at a time (a full adjoint is not provided).
+
+``RoeExnerSteps`` wraps the run as a ``torch.autograd.Function`` with a forward-mode
+rule, so ``torch.autograd.forward_ad`` dual tensors flow through it.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+import torch.autograd.forward_ad as fwAD
+
+from . import _lib
+from .solvers import _re_plan, _stream
+from .state import RoeExnerState, alloc_plane
+
+
+def _check(state, state_dot):
+    if state.dtype != torch.float64 or state_dot.dtype != torch.float64:
+        raise ValueError("the tangent-linear model runs in float64")
+    state.check_layout()
+    state_dot.check_layout()
+    if state_dot.pitch != state.pitch or state_dot.shape != state.shape:
+        raise ValueError("state and tangent must share shape and pitch")
+
+
+def jvp_init(state, state_dot, mask, solver_config):
+    """init_fn_roeexner and its tangent (on copies): returns (state, state_dot)."""
+    _check(state, state_dot)
+    s, t = state.clone(), state_dot.clone()
+    plan = _re_plan(s, mask, solver_config)
+    _lib.call("pxb_re_jvp_init", plan.handle, ctypes.byref(s.c_fields()), ctypes.byref(t.c_fields()), _stream())
+    return s, t
+
+
+def jvp_run(state, state_dot, mask, solver_config, n_steps, scheme="SSPRK2", cfl=0.5, t0=0.0):
+    """Advance ``state`` and ``state_dot`` IN PLACE by ``n_steps`` steps; returns the dts
+    and their tangents as float64 device tensors."""
+    _check(state, state_dot)
+    plan = _re_plan(state, mask, solver_config)
+    dev = state.h.device
+    dts = torch.empty(max(1, n_steps), dtype=torch.float64, device=dev)
+    dts_dot = torch.empty(max(1, n_steps), dtype=torch.float64, device=dev)
+    code = _lib.SSPRK2 if scheme == "SSPRK2" else _lib.FE
+    _lib.call("pxb_re_jvp_run", plan.handle, ctypes.byref(state.c_fields()), ctypes.byref(state_dot.c_fields()),
+              int(n_steps), code, float(cfl), float(t0), ctypes.c_void_p(dts.data_ptr()),
+              ctypes.c_void_p(dts_dot.data_ptr()), _stream())
+    return dts[:n_steps], dts_dot[:n_steps]
+
+
+class StepsSpec:
+    """What ``RoeExnerSteps`` runs: mask, solver config, sediment matrix, step count,
+    scheme and CFL number."""
+
+    def __init__(self, mask, solver_config, seds, n_steps, scheme="SSPRK2", cfl=0.5):
+        self.mask, self.cfg, self.seds = mask, solver_config, seds
+        self.n_steps, self.scheme, self.cfl = int(n_steps), scheme, float(cfl)
+
+
+def _state_from(planes, seds):
+    ny, nx = planes[0].shape
+    kw = {}
+    for f, p in zip(RoeExnerState.PLANES, planes):
+        t = alloc_plane(ny, nx, torch.float64, planes[0].device)
+        t.copy_(p)
+        kw[f] = t
+    return RoeExnerState(**kw, seds=seds)
+
+
+class RoeExnerSteps(torch.autograd.Function):
+    """``spec.n_steps`` fixed steps of the float64 Roe-Exner bundle as a differentiable
+    function of the eight state planes (h, hu, hv, z, z_b, n, n_b, G), forward mode only:
+
+        with fwAD.dual_level():
+            planes = [fwAD.make_dual(p, t) for p, t in zip(planes, tangents)]
+            out = RoeExnerSteps.apply(spec, *planes)
+            tangents_out = [fwAD.unpack_dual(o).tangent for o in out]
+    """
+
+    @staticmethod
+    def forward(ctx, spec, *planes):
+        from .integrators import run_steps
+
+        ctx.spec = spec
+        ctx.save_for_forward(*planes)
+        st = _state_from(planes, spec.seds)
+        run_steps(st, spec.mask, spec.cfg, spec.scheme, spec.n_steps, spec.cfl, log_dt=False)
+        return tuple(getattr(st, f).clone() for f in RoeExnerState.PLANES)
+
+    @staticmethod
+    def jvp(ctx, _spec_tangent, *tangents):
+        spec = ctx.spec
+        planes = ctx.saved_tensors
+        st = _state_from(planes, spec.seds)
+        td = _state_from([t if t is not None else torch.zeros_like(p) for t, p in zip(tangents, planes)], spec.seds)
+        jvp_run(st, td, spec.mask, spec.cfg, spec.n_steps, spec.scheme, spec.cfl)
+        return tuple(getattr(td, f).clone() for f in RoeExnerState.PLANES)
+
+    @staticmethod
+    def backward(ctx, *grads):
+        raise NotImplementedError("RoeExnerSteps provides forward-mode derivatives only")
+
+
+__all__ = ["jvp_init", "jvp_run", "RoeExnerSteps", "StepsSpec", "fwAD"]
