@@ -23,9 +23,15 @@
 
 #include "pxb_device.cuh"
 
-// Resident 128-thread blocks per SM the float build is register-limited to (tuning knob).
+// Resident 128-thread blocks per SM the build is register-limited to (tuning knobs,
+// measured on the 2048^2 and 8192^2 Gaussian-bed cases): 4 (128 registers, no spills)
+// for the plain stage; 5 (96 registers) for the averaging second SSPRK2 stage, whose
+// partner-state loads want the extra warps to hide their latency.
 #ifndef PXB_STAGE_MIN_BLOCKS
-#define PXB_STAGE_MIN_BLOCKS 5
+#define PXB_STAGE_MIN_BLOCKS 4
+#endif
+#ifndef PXB_STAGE_MIN_BLOCKS_AVG
+#define PXB_STAGE_MIN_BLOCKS_AVG 5
 #endif
 
 namespace pxb {
@@ -149,10 +155,31 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
             const T h_r = nh, hu_r = nhu, hv_r = nhv, zb_r = nzb, z_r = nz, nb_r = nnb, g_r = ng;
             const bool m_r = nm;
             load_row(r + 1);
+            // SSPRK2 partner values of the cells stored at the end of this iteration (rows
+            // r-3 and r-5), loaded here so that their latency hides behind the arithmetic.
+            // Only the owning lane reads and then writes these cells, so this is safe when
+            // the output aliases the partner.
+            T pah = 0, pahu = 0, pahv = 0, pazb = 0, paG = 0;
+            if (AVG) {
+                const int q0 = r - 3, p0 = r - 5;
+                if ((S || (q0 >= L0 && q0 < L1)) && q0 >= R0 && q0 < R1 && out_col) {
+                    const unsigned i = (unsigned)q0 * upitch + (unsigned)c;
+                    pah = a.ah[i];
+                    pahu = a.ahu[i];
+                    pahv = a.ahv[i];
+                }
+                if ((S || (p0 >= L0 && p0 < L1)) && p0 >= R0 && p0 < R1 && out_col) {
+                    const unsigned i = (unsigned)p0 * upitch + (unsigned)c;
+                    pazb = a.azb[i];
+                    if (a.oG) paG = a.aG[i];
+                }
+            }
             const HCell<T> pr = make_hcell(h_r, hu_r, hv_r, zb_r, z_r, nb_r);
             const T zt_r = z_r + zb_r;
             T xf0 = 0, xf1 = 0, xf2 = 0;
-            {
+            // In the prologue / drain iterations of a band the faces of invalid rows are
+            // skipped for the whole warp (r is warp-uniform); their results would be masked.
+            if (S || rowA) {
                 const HCell<T> pe = shfl_down_hcell(pr);
                 const T he = __shfl_down_sync(FULL, h_r, 1);
                 const bool me = HAS_MASK ? (__shfl_down_sync(FULL, (int)m_r, 1) != 0) : false;
@@ -169,11 +196,13 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
                 if (xact) { xf0 = xf0 + M[0]; xf1 = xf1 + M[1]; xf2 = xf2 + M[2]; }
                 if (wact) { xf0 = xf0 + w0; xf1 = xf1 + w1; xf2 = xf2 + w2; }
             }
-            T yP[3], yM[3];
+            T yP[3] = {T(0), T(0), T(0)}, yM[3] = {T(0), T(0), T(0)};
             const bool yact = rowA && (S || r - 1 >= L0) && colok && ((hA > DRY) || (h_r > DRY)) && !((mwin & 1u) || m_r);
-            roe_exner_face<T, true>(pA, pr, dx, yP, yM);
+            if (S || (rowA && r - 1 >= L0)) {
+                roe_exner_face<T, true>(pA, pr, dx, yP, yM);
 #pragma unroll
-            for (int k = 0; k < 3; ++k) { yP[k] = yact ? yP[k] : T(0); yM[k] = yact ? yM[k] : T(0); }
+                for (int k = 0; k < 3; ++k) { yP[k] = yact ? yP[k] : T(0); yM[k] = yact ? yM[k] : T(0); }
+            }
 
             // ================= B: hydro update of row r-1
             T hr1 = 0, hur1 = 0, hvr1 = 0;
@@ -279,9 +308,11 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
             // ================= E: grass factor, Exner cell and faces of row q
             const bool mq = HAS_MASK && ((mwin >> 2) & 1u);
             const bool mq1 = HAS_MASK && ((mwin >> 3) & 1u);
+            ECell<T> e3{};
+            T xe3 = 0, Fy = 0;
+            if (S || rowD) {  // warp-uniform: row q is outside the band's rows in some prologue / drain iterations
             const T Gq = MPM ? mpm_grass(hbh, hbu, hbv, mq, a.sed) : const_grass(hbh, gb1, mq);
-            const ECell<T> e3 = make_ecell(hbh, hbu, hbv, zb1, Gq);
-            T xe3 = 0;
+            e3 = make_ecell(hbh, hbu, hbv, zb1, Gq);
             {
                 const ECell<T> ee = shfl_down_ecell(e3);
                 const bool mqe = HAS_MASK ? (__shfl_down_sync(FULL, (int)mq, 1) != 0) : false;
@@ -296,7 +327,8 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
             }
             const bool yex = rowD && (S || q - 1 >= L0) && colok && exner_active(e4, e3, mq1, mq);
             const T Fyv = exner_face<T, true>(e4, e3);
-            const T Fy = yex ? Fyv : T(0);
+            Fy = yex ? Fyv : T(0);
+            }
 
             // ================= F: z_b update of row r-4
             T zbp4 = 0;
@@ -334,8 +366,8 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
             if (rowG && p >= R0 && p < R1 && out_col) {
                 const unsigned i = (unsigned)p * upitch + (unsigned)c;
                 if (AVG) {
-                    zfin = T(0.5) * a.azb[i] + T(0.5) * zfin;
-                    if (a.oG) gfin = T(0.5) * a.aG[i] + T(0.5) * gfin;
+                    zfin = T(0.5) * pazb + T(0.5) * zfin;
+                    if (a.oG) gfin = T(0.5) * paG + T(0.5) * gfin;
                 }
                 a.ozb[i] = zfin;
                 if (a.oG) a.oG[i] = gfin;
@@ -345,9 +377,9 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
                 const unsigned i = (unsigned)q * upitch + (unsigned)c;
                 T oh = sbh, ou = sbu, ov = sbv;
                 if (AVG) {
-                    oh = T(0.5) * a.ah[i] + T(0.5) * oh;
-                    ou = T(0.5) * a.ahu[i] + T(0.5) * ou;
-                    ov = T(0.5) * a.ahv[i] + T(0.5) * ov;
+                    oh = T(0.5) * pah + T(0.5) * oh;
+                    ou = T(0.5) * pahu + T(0.5) * ou;
+                    ov = T(0.5) * pahv + T(0.5) * ov;
                 }
                 a.oh[i] = oh;
                 a.ohu[i] = ou;
@@ -379,7 +411,8 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
 }
 
 template <class T, bool MPM, bool HAS_MASK, bool AVG>
-__global__ void __launch_bounds__(128, PXB_STAGE_MIN_BLOCKS) re_stage_kernel(const REStageArgs<T> a) {
+__global__ void __launch_bounds__(128, AVG ? PXB_STAGE_MIN_BLOCKS_AVG : PXB_STAGE_MIN_BLOCKS)
+    re_stage_kernel(const REStageArgs<T> a) {
     const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     const int nitems = a.nstrips * a.nbands;
