@@ -6,8 +6,10 @@
 // handlers, and for the second SSPRK2 stage the 0.5/0.5 combination (SSPRK2.py:40).
 //
 // Layout of the work: a warp owns a strip of 32 columns (3 halo | 26 owned | 3 halo) and
-// marches down a band of rows.  Each iteration loads one new row and advances a
-// software pipeline held in registers:
+// marches down a band of rows.  Each iteration consumes one new row, copied into the
+// warp's shared buffer by cp.async during the previous iteration (together with the
+// partner-state values the averaging stage stores in this one), and advances a software
+// pipeline held in registers:
 //   A  row r   : cell precompute, x-face fluxes (east neighbour by shuffle), y-face (r-1|r)
 //   B  row r-1 : hydro update (all four faces known)
 //   C  row r-2 : momentum corrections (needs updated depths of rows r-3..r-1)
@@ -24,11 +26,10 @@
 #include "pxb_device.cuh"
 
 // Resident 128-thread blocks per SM the build is register-limited to (tuning knobs,
-// measured on the 2048^2 and 8192^2 Gaussian-bed cases): 4 (128 registers, no spills)
-// for the plain stage; 5 (96 registers) for the averaging second SSPRK2 stage, whose
-// partner-state loads want the extra warps to hide their latency.
+// measured on the 2048^2 and 8192^2 Gaussian-bed cases): 5 (96 registers) for both the
+// plain stage and the averaging second SSPRK2 stage.
 #ifndef PXB_STAGE_MIN_BLOCKS
-#define PXB_STAGE_MIN_BLOCKS 4
+#define PXB_STAGE_MIN_BLOCKS 5
 #endif
 #ifndef PXB_STAGE_MIN_BLOCKS_AVG
 #define PXB_STAGE_MIN_BLOCKS_AVG 5
@@ -51,6 +52,17 @@ struct REStageArgs {
     int band_rows, nstrips, nbands;
     int* err;
 };
+
+// Asynchronous global -> shared copies of one element (cp.async, completion by group).
+template <class T>
+__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    if constexpr (sizeof(T) == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 template <class T>
 __device__ __forceinline__ T pick_row(int dy, T above, T mid, T below) {
@@ -124,27 +136,56 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
         T xe4 = 0, fn4 = 0;
         T zbp6 = 0, zbp5 = 0, gg6 = 0, gg5 = 0;
 
-        // row r+1 is loaded while row r is computed (the loads of one iteration are in
-        // flight during the ~thousand instructions of the previous one)
-        T nh = 0, nhu = 0, nhv = 0, nzb = 0, nz = 0, nnb = 0, ng = 0;
+        // Row r+1 is copied asynchronously (cp.async) into this warp's shared buffer while
+        // row r is computed: the copies of one iteration are in flight during the
+        // ~thousand instructions of the previous one and hold no registers meanwhile.
+        constexpr int NP = MPM ? 6 : 7;
+        __shared__ T rbuf[4][2][NP][32];
+        T(*rb)[NP][32] = rbuf[threadIdx.x >> 5];
         bool nm = false;
         auto load_row = [&](int rr) {
+            const int b = rr & 1;
             if (rr < L1 && colok) {
                 const unsigned i = (unsigned)rr * upitch + (unsigned)c;
-                nh = __ldg(a.h + i);
-                nhu = __ldg(a.hu + i);
-                nhv = __ldg(a.hv + i);
-                nzb = __ldg(a.zb + i);
-                nz = __ldg(a.z + i);
-                nnb = __ldg(a.nb + i);
-                if (!MPM) ng = __ldg(a.G + i);
+                cp_async_elem(&rb[b][0][lane], a.h + i);
+                cp_async_elem(&rb[b][1][lane], a.hu + i);
+                cp_async_elem(&rb[b][2][lane], a.hv + i);
+                cp_async_elem(&rb[b][3][lane], a.zb + i);
+                cp_async_elem(&rb[b][4][lane], a.z + i);
+                cp_async_elem(&rb[b][5][lane], a.nb + i);
+                if constexpr (!MPM) cp_async_elem(&rb[b][NP - 1][lane], a.G + i);
                 if (HAS_MASK) nm = __ldg(a.nodata + i) != 0;
             } else {
-                nh = nhu = nhv = nzb = nz = nnb = ng = T(0);
+#pragma unroll
+                for (int k = 0; k < NP; ++k) rb[b][k][lane] = T(0);
                 nm = false;
             }
         };
         load_row(L0);
+        // Averaging stage: the partner state's values of the cells stored in iteration r
+        // (rows r-3 and r-5) are copied asynchronously into this warp's shared buffer
+        // during iteration r-1, so they cost neither registers nor a wait at the store.
+        // Only the owning lane reads and then writes these cells, so this is safe when the
+        // output aliases the partner.
+        __shared__ T pbuf[4][2][5][32];
+        T(*pb)[5][32] = pbuf[threadIdx.x >> 5];
+        auto partner_copy = [&](const int rr) {  // the rows stored in iteration rr
+            const int q0 = rr - 3, p0 = rr - 5;
+            const int b = rr & 1;
+            if (q0 >= L0 && q0 < L1 && q0 >= R0 && q0 < R1 && out_col) {
+                const unsigned i = (unsigned)q0 * upitch + (unsigned)c;
+                cp_async_elem(&pb[b][0][lane], a.ah + i);
+                cp_async_elem(&pb[b][1][lane], a.ahu + i);
+                cp_async_elem(&pb[b][2][lane], a.ahv + i);
+            }
+            if (p0 >= L0 && p0 < L1 && p0 >= R0 && p0 < R1 && out_col) {
+                const unsigned i = (unsigned)p0 * upitch + (unsigned)c;
+                cp_async_elem(&pb[b][3][lane], a.azb + i);
+                if (a.oG) cp_async_elem(&pb[b][4][lane], a.aG + i);
+            }
+        };
+        if (AVG) partner_copy(L0);
+        cp_async_commit();
 
         // One pipeline iteration.  In the steady state (rows L0+5 .. L1-1) every phase has
         // valid rows, so the row checks compile away.
@@ -152,28 +193,16 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
             constexpr bool S = decltype(steady_tag)::value;
             const bool rowA = S || r < L1;
             // ================= A: row r (prefetched), x-faces of row r, y-face (r-1 | r)
-            const T h_r = nh, hu_r = nhu, hv_r = nhv, zb_r = nzb, z_r = nz, nb_r = nnb, g_r = ng;
+            cp_async_wait<0>();  // row r (and the partner rows stored in this iteration)
+            const int rbb = r & 1;
+            const T h_r = rb[rbb][0][lane], hu_r = rb[rbb][1][lane], hv_r = rb[rbb][2][lane];
+            const T zb_r = rb[rbb][3][lane], z_r = rb[rbb][4][lane], nb_r = rb[rbb][5][lane];
+            T g_r = T(0);
+            if constexpr (!MPM) g_r = rb[rbb][NP - 1][lane];
             const bool m_r = nm;
             load_row(r + 1);
-            // SSPRK2 partner values of the cells stored at the end of this iteration (rows
-            // r-3 and r-5), loaded here so that their latency hides behind the arithmetic.
-            // Only the owning lane reads and then writes these cells, so this is safe when
-            // the output aliases the partner.
-            T pah = 0, pahu = 0, pahv = 0, pazb = 0, paG = 0;
-            if (AVG) {
-                const int q0 = r - 3, p0 = r - 5;
-                if ((S || (q0 >= L0 && q0 < L1)) && q0 >= R0 && q0 < R1 && out_col) {
-                    const unsigned i = (unsigned)q0 * upitch + (unsigned)c;
-                    pah = a.ah[i];
-                    pahu = a.ahu[i];
-                    pahv = a.ahv[i];
-                }
-                if ((S || (p0 >= L0 && p0 < L1)) && p0 >= R0 && p0 < R1 && out_col) {
-                    const unsigned i = (unsigned)p0 * upitch + (unsigned)c;
-                    pazb = a.azb[i];
-                    if (a.oG) paG = a.aG[i];
-                }
-            }
+            if (AVG) partner_copy(r + 1);
+            cp_async_commit();
             const HCell<T> pr = make_hcell(h_r, hu_r, hv_r, zb_r, z_r, nb_r);
             const T zt_r = z_r + zb_r;
             T xf0 = 0, xf1 = 0, xf2 = 0;
@@ -366,8 +395,8 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
             if (rowG && p >= R0 && p < R1 && out_col) {
                 const unsigned i = (unsigned)p * upitch + (unsigned)c;
                 if (AVG) {
-                    zfin = T(0.5) * pazb + T(0.5) * zfin;
-                    if (a.oG) gfin = T(0.5) * paG + T(0.5) * gfin;
+                    zfin = T(0.5) * pb[r & 1][3][lane] + T(0.5) * zfin;
+                    if (a.oG) gfin = T(0.5) * pb[r & 1][4][lane] + T(0.5) * gfin;
                 }
                 a.ozb[i] = zfin;
                 if (a.oG) a.oG[i] = gfin;
@@ -377,9 +406,9 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
                 const unsigned i = (unsigned)q * upitch + (unsigned)c;
                 T oh = sbh, ou = sbu, ov = sbv;
                 if (AVG) {
-                    oh = T(0.5) * pah + T(0.5) * oh;
-                    ou = T(0.5) * pahu + T(0.5) * ou;
-                    ov = T(0.5) * pahv + T(0.5) * ov;
+                    oh = T(0.5) * pb[r & 1][0][lane] + T(0.5) * oh;
+                    ou = T(0.5) * pb[r & 1][1][lane] + T(0.5) * ou;
+                    ov = T(0.5) * pb[r & 1][2][lane] + T(0.5) * ov;
                 }
                 a.oh[i] = oh;
                 a.ohu[i] = ou;
@@ -407,6 +436,7 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
         for (; r < steady0; ++r) iterate(r, std::false_type{});
         for (; r < steady1; ++r) iterate(r, std::true_type{});
         for (; r < L1 + 5; ++r) iterate(r, std::false_type{});
+        cp_async_wait<0>();  // the buffers are reused by the next item
     }
 }
 
