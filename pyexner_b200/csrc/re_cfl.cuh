@@ -64,17 +64,28 @@ __device__ __forceinline__ void re_cfl_item(const CflArgs<T>& a, const int item,
         CCell<T> prev = make_ccell(T(1), T(0), T(0), T(0));
         T hprev = 0;
         bool mprev = false;
-        for (int r = R0; r < min(ny, R1 + 1); ++r) {
-            T h = 1, hu = 0, hv = 0, g = 0;
-            bool m = false;
-            if (colok) {
-                const long long i = (long long)r * a.pitch + c;
-                h = a.h[i];
-                hu = a.hu[i];
-                hv = a.hv[i];
-                g = a.G[i];
-                if (HAS_MASK) m = a.nodata[i] != 0;
+        const int rend = min(ny, R1 + 1);
+        // row r+1 is loaded while row r is evaluated
+        T nh = 1, nhu = 0, nhv = 0, ng = 0;
+        bool nm = false;
+        auto fetch = [&](int rr) {
+            nh = 1;
+            nhu = nhv = ng = 0;
+            nm = false;
+            if (colok && rr < rend) {
+                const long long i = (long long)rr * a.pitch + c;
+                nh = __ldg(a.h + i);
+                nhu = __ldg(a.hu + i);
+                nhv = __ldg(a.hv + i);
+                ng = __ldg(a.G + i);
+                if (HAS_MASK) nm = __ldg(a.nodata + i) != 0;
             }
+        };
+        fetch(R0);
+        for (int r = R0; r < rend; ++r) {
+            const T h = nh, hu = nhu, hv = nhv, g = ng;
+            const bool m = nm;
+            fetch(r + 1);
             const CCell<T> cur = make_ccell(h, hu, hv, g);
             if (r < R1) {  // x-face (c | c+1) of row r
                 CCell<T> e;
