@@ -55,8 +55,7 @@ __device__ __forceinline__ void ens_load_slot(A* slot, const A* src) {
 }
 
 template <class T, bool MPM, bool HAS_MASK, bool AVG>
-__global__ void __launch_bounds__(128, AVG ? PXB_STAGE_MIN_BLOCKS_AVG : PXB_STAGE_MIN_BLOCKS)
-    ens_stage_kernel(const EnsStageArgs<T> e) {
+__global__ void __launch_bounds__(128, PXB_STAGE_BOUNDS(T, AVG)) ens_stage_kernel(const EnsStageArgs<T> e) {
     __shared__ REStageArgs<T> slot[4];
     const int w = threadIdx.x >> 5;
     const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;

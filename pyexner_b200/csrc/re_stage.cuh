@@ -34,6 +34,12 @@
 #ifndef PXB_STAGE_MIN_BLOCKS_AVG
 #define PXB_STAGE_MIN_BLOCKS_AVG 5
 #endif
+// float64 state (twice the registers per value)
+#ifndef PXB_STAGE_MIN_BLOCKS_F64
+#define PXB_STAGE_MIN_BLOCKS_F64 5
+#endif
+#define PXB_STAGE_BOUNDS(T, AVG) \
+    (sizeof(T) == 8 ? PXB_STAGE_MIN_BLOCKS_F64 : ((AVG) ? PXB_STAGE_MIN_BLOCKS_AVG : PXB_STAGE_MIN_BLOCKS))
 
 namespace pxb {
 
@@ -136,38 +142,61 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
         T xe4 = 0, fn4 = 0;
         T zbp6 = 0, zbp5 = 0, gg6 = 0, gg5 = 0;
 
-        // Row r+1 is copied asynchronously (cp.async) into this warp's shared buffer while
-        // row r is computed: the copies of one iteration are in flight during the
-        // ~thousand instructions of the previous one and hold no registers meanwhile.
+        // Row r+1 is fetched while row r is computed: the loads of one iteration are in
+        // flight during the ~thousand instructions of the previous one.  In float32 they
+        // are cp.async copies into this warp's shared buffer (no registers held); in
+        // float64 (measured: faster there) plain loads into registers.
+        constexpr bool ASYNC_ROWS = is_f32<T>();
         constexpr int NP = MPM ? 6 : 7;
-        __shared__ T rbuf[4][2][NP][32];
-        T(*rb)[NP][32] = rbuf[threadIdx.x >> 5];
+        __shared__ T rbuf[4][ASYNC_ROWS ? 2 : 1][ASYNC_ROWS ? NP : 1][32];
+        T(*rb)[ASYNC_ROWS ? NP : 1][32] = rbuf[threadIdx.x >> 5];
+        T nh = 0, nhu = 0, nhv = 0, nzb = 0, nz = 0, nnb = 0, ng = 0;
         bool nm = false;
         auto load_row = [&](int rr) {
             const int b = rr & 1;
-            if (rr < L1 && colok) {
-                const unsigned i = (unsigned)rr * upitch + (unsigned)c;
-                cp_async_elem(&rb[b][0][lane], a.h + i);
-                cp_async_elem(&rb[b][1][lane], a.hu + i);
-                cp_async_elem(&rb[b][2][lane], a.hv + i);
-                cp_async_elem(&rb[b][3][lane], a.zb + i);
-                cp_async_elem(&rb[b][4][lane], a.z + i);
-                cp_async_elem(&rb[b][5][lane], a.nb + i);
-                if constexpr (!MPM) cp_async_elem(&rb[b][NP - 1][lane], a.G + i);
-                if (HAS_MASK) nm = __ldg(a.nodata + i) != 0;
+            if constexpr (!ASYNC_ROWS) {
+                if (rr < L1 && colok) {
+                    const unsigned i = (unsigned)rr * upitch + (unsigned)c;
+                    nh = __ldg(a.h + i);
+                    nhu = __ldg(a.hu + i);
+                    nhv = __ldg(a.hv + i);
+                    nzb = __ldg(a.zb + i);
+                    nz = __ldg(a.z + i);
+                    nnb = __ldg(a.nb + i);
+                    if (!MPM) ng = __ldg(a.G + i);
+                    if (HAS_MASK) nm = __ldg(a.nodata + i) != 0;
+                } else {
+                    nh = nhu = nhv = nzb = nz = nnb = ng = T(0);
+                    nm = false;
+                }
             } else {
+                if (rr < L1 && colok) {
+                    const unsigned i = (unsigned)rr * upitch + (unsigned)c;
+                    cp_async_elem(&rb[b][0][lane], a.h + i);
+                    cp_async_elem(&rb[b][1][lane], a.hu + i);
+                    cp_async_elem(&rb[b][2][lane], a.hv + i);
+                    cp_async_elem(&rb[b][3][lane], a.zb + i);
+                    cp_async_elem(&rb[b][4][lane], a.z + i);
+                    cp_async_elem(&rb[b][5][lane], a.nb + i);
+                    if constexpr (!MPM) cp_async_elem(&rb[b][NP - 1][lane], a.G + i);
+                    if (HAS_MASK) nm = __ldg(a.nodata + i) != 0;
+                } else {
 #pragma unroll
-                for (int k = 0; k < NP; ++k) rb[b][k][lane] = T(0);
-                nm = false;
+                    for (int k = 0; k < NP; ++k) rb[b][k][lane] = T(0);
+                    nm = false;
+                }
             }
         };
         load_row(L0);
         // Averaging stage: the partner state's values of the cells stored in iteration r
-        // (rows r-3 and r-5) are copied asynchronously into this warp's shared buffer
-        // during iteration r-1, so they cost neither registers nor a wait at the store.
-        // Only the owning lane reads and then writes these cells, so this is safe when the
-        // output aliases the partner.
-        __shared__ T pbuf[4][2][5][32];
+        // (rows r-3 and r-5).  In float32 they are copied asynchronously into this warp's
+        // shared buffer during iteration r-1, so they cost neither registers nor a wait at
+        // the store; in float64 (measured: the shared-buffer form is slower there) they
+        // are loaded into registers at the start of iteration r.  Only the owning lane
+        // reads and then writes these cells, so both are safe when the output aliases the
+        // partner.
+        constexpr bool ASYNC_PARTNER = AVG && is_f32<T>();
+        __shared__ T pbuf[4][ASYNC_PARTNER ? 2 : 1][5][32];
         T(*pb)[5][32] = pbuf[threadIdx.x >> 5];
         auto partner_copy = [&](const int rr) {  // the rows stored in iteration rr
             const int q0 = rr - 3, p0 = rr - 5;
@@ -184,7 +213,7 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
                 if (a.oG) cp_async_elem(&pb[b][4][lane], a.aG + i);
             }
         };
-        if (AVG) partner_copy(L0);
+        if (ASYNC_PARTNER) partner_copy(L0);
         cp_async_commit();
 
         // One pipeline iteration.  In the steady state (rows L0+5 .. L1-1) every phase has
@@ -193,16 +222,41 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
             constexpr bool S = decltype(steady_tag)::value;
             const bool rowA = S || r < L1;
             // ================= A: row r (prefetched), x-faces of row r, y-face (r-1 | r)
-            cp_async_wait<0>();  // row r (and the partner rows stored in this iteration)
-            const int rbb = r & 1;
-            const T h_r = rb[rbb][0][lane], hu_r = rb[rbb][1][lane], hv_r = rb[rbb][2][lane];
-            const T zb_r = rb[rbb][3][lane], z_r = rb[rbb][4][lane], nb_r = rb[rbb][5][lane];
-            T g_r = T(0);
-            if constexpr (!MPM) g_r = rb[rbb][NP - 1][lane];
+            T h_r, hu_r, hv_r, zb_r, z_r, nb_r, g_r = T(0);
+            if constexpr (ASYNC_ROWS) {
+                cp_async_wait<0>();  // row r (and the partner rows stored in this iteration)
+                const int rbb = r & 1;
+                h_r = rb[rbb][0][lane];
+                hu_r = rb[rbb][1][lane];
+                hv_r = rb[rbb][2][lane];
+                zb_r = rb[rbb][3][lane];
+                z_r = rb[rbb][4][lane];
+                nb_r = rb[rbb][5][lane];
+                if constexpr (!MPM) g_r = rb[rbb][NP - 1][lane];
+            } else {
+                h_r = nh, hu_r = nhu, hv_r = nhv, zb_r = nzb, z_r = nz, nb_r = nnb, g_r = ng;
+            }
             const bool m_r = nm;
             load_row(r + 1);
-            if (AVG) partner_copy(r + 1);
+            if (ASYNC_PARTNER) partner_copy(r + 1);
             cp_async_commit();
+            T pah = 0, pahu = 0, pahv = 0, pazb = 0, paG = 0;
+            if (ASYNC_PARTNER) {
+                // read at the stores below
+            } else if (AVG) {
+                const int q0 = r - 3, p0 = r - 5;
+                if ((S || (q0 >= L0 && q0 < L1)) && q0 >= R0 && q0 < R1 && out_col) {
+                    const unsigned i = (unsigned)q0 * upitch + (unsigned)c;
+                    pah = a.ah[i];
+                    pahu = a.ahu[i];
+                    pahv = a.ahv[i];
+                }
+                if ((S || (p0 >= L0 && p0 < L1)) && p0 >= R0 && p0 < R1 && out_col) {
+                    const unsigned i = (unsigned)p0 * upitch + (unsigned)c;
+                    pazb = a.azb[i];
+                    if (a.oG) paG = a.aG[i];
+                }
+            }
             const HCell<T> pr = make_hcell(h_r, hu_r, hv_r, zb_r, z_r, nb_r);
             const T zt_r = z_r + zb_r;
             T xf0 = 0, xf1 = 0, xf2 = 0;
@@ -395,8 +449,12 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
             if (rowG && p >= R0 && p < R1 && out_col) {
                 const unsigned i = (unsigned)p * upitch + (unsigned)c;
                 if (AVG) {
-                    zfin = T(0.5) * pb[r & 1][3][lane] + T(0.5) * zfin;
-                    if (a.oG) gfin = T(0.5) * pb[r & 1][4][lane] + T(0.5) * gfin;
+                    if (ASYNC_PARTNER) {
+                        pazb = pb[r & 1][3][lane];
+                        if (a.oG) paG = pb[r & 1][4][lane];
+                    }
+                    zfin = T(0.5) * pazb + T(0.5) * zfin;
+                    if (a.oG) gfin = T(0.5) * paG + T(0.5) * gfin;
                 }
                 a.ozb[i] = zfin;
                 if (a.oG) a.oG[i] = gfin;
@@ -406,9 +464,14 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
                 const unsigned i = (unsigned)q * upitch + (unsigned)c;
                 T oh = sbh, ou = sbu, ov = sbv;
                 if (AVG) {
-                    oh = T(0.5) * pb[r & 1][0][lane] + T(0.5) * oh;
-                    ou = T(0.5) * pb[r & 1][1][lane] + T(0.5) * ou;
-                    ov = T(0.5) * pb[r & 1][2][lane] + T(0.5) * ov;
+                    if (ASYNC_PARTNER) {
+                        pah = pb[r & 1][0][lane];
+                        pahu = pb[r & 1][1][lane];
+                        pahv = pb[r & 1][2][lane];
+                    }
+                    oh = T(0.5) * pah + T(0.5) * oh;
+                    ou = T(0.5) * pahu + T(0.5) * ou;
+                    ov = T(0.5) * pahv + T(0.5) * ov;
                 }
                 a.oh[i] = oh;
                 a.ohu[i] = ou;
@@ -441,8 +504,7 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
 }
 
 template <class T, bool MPM, bool HAS_MASK, bool AVG>
-__global__ void __launch_bounds__(128, AVG ? PXB_STAGE_MIN_BLOCKS_AVG : PXB_STAGE_MIN_BLOCKS)
-    re_stage_kernel(const REStageArgs<T> a) {
+__global__ void __launch_bounds__(128, PXB_STAGE_BOUNDS(T, AVG)) re_stage_kernel(const REStageArgs<T> a) {
     const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     const int nitems = a.nstrips * a.nbands;
