@@ -10,8 +10,9 @@ Reported:
   value      cell-updates/s of the device loop (graph replay), state resident in HBM,
              L2 flushed (256 MiB write) between timed steps and excluded from the timing;
   e2e        the same metric through the public API with host buffers: pinned-host ->
-             device copy of the state, ``run_steps`` for all K steps, device -> host copy
-             of the state, all inside the timed region;
+             device copy of the state, init, ``run_steps`` for all K steps, device -> host
+             copy of the state, all inside the timed region (the second such call: the
+             first, untimed, warms the allocator and captures the step graph);
   roofline   the stage kernels' algorithmic bytes per launch over their CUDA-event
              duration, against the measured HBM copy bandwidth;
   fp64       the same loop in float64 (the plain FP64 GPU path) and its speed ratio;
@@ -264,15 +265,21 @@ def e2e_run(n, dtype, steps, warmup):
     run_steps(st, mask, cfg, "SSPRK2", warmup, 0.5)
     torch.cuda.synchronize()
     stream = torch.cuda.current_stream()
+
+    def call():
+        for k in planes:
+            getattr(st, k).copy_(host[k], non_blocking=True)
+        st2 = bundle.init_fn(st, mask, cfg)
+        run_steps(st2, mask, cfg, "SSPRK2", steps, 0.5, log_dt=False)
+        for k in out:
+            out[k].copy_(getattr(st2, k), non_blocking=True)
+
+    call()  # untimed: warms the allocator and captures the step graph for these buffers
+    torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for k in planes:
-        getattr(st, k).copy_(host[k], non_blocking=True)
-    st2 = bundle.init_fn(st, mask, cfg)
-    run_steps(st2, mask, cfg, "SSPRK2", steps, 0.5, log_dt=False)
-    for k in out:
-        out[k].copy_(getattr(st2, k), non_blocking=True)
+    call()
     e1.record(stream)
     e1.synchronize()
     sec = e0.elapsed_time(e1) / 1e3
@@ -539,7 +546,8 @@ def main():
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
                 "d2h_bytes_per_step": d2h / args.steps,
-                "note": "pinned host state -> device, init + K steps via run_steps, final state -> host"},
+                "note": "pinned host state -> device, init + K steps via run_steps, final state -> host "
+                        "(second call; the first, untimed, warms the allocator and the step graph)"},
         "gpu_launches": 3 * args.steps,
         "clocks": clk.summary(),
     }
