@@ -189,11 +189,20 @@ int pxb_re_run(pxb_re_plan* plan, const pxb_re_fields* a, const pxb_re_fields* b
  * values bit for bit as the float64 run, tangents by the chain rule through the step
  * including the state dependence of dt through the fastest face.  The stage runs the
  * general path's kernels on dual numbers (any boundary layout); the plan allocates its
- * dual planes on the first call.  dt_log / dt_dot_log: device float64 arrays of nsteps
- * values / tangents of dt, or NULL. */
-int pxb_re_jvp_init(pxb_re_plan* plan, const pxb_re_fields* f, const pxb_re_fields* f_dot, void* stream);
+ * dual planes on the first call.  Parameter tangents (may be NULL, or have NULL members):
+ * seds_dot, 7 x nsed like pxb_re_config.seds (the MPM constants follow); values0_dot, one
+ * per handler in plan order, the tangent of values[0] of ConstantInflux handlers (the
+ * discharge; its momenta are q * values[1], q * values[2]).  dt_log / dt_dot_log: device
+ * float64 arrays of nsteps values / tangents of dt, or NULL. */
+typedef struct pxb_re_tangent_params {
+    const double* seds_dot;
+    const double* values0_dot;
+} pxb_re_tangent_params;
+int pxb_re_jvp_init(pxb_re_plan* plan, const pxb_re_fields* f, const pxb_re_fields* f_dot,
+                    const pxb_re_tangent_params* params_dot, void* stream);
 int pxb_re_jvp_run(pxb_re_plan* plan, const pxb_re_fields* a, const pxb_re_fields* a_dot, int32_t nsteps,
-                   int32_t scheme, double cfl, double t0, void* dt_log, void* dt_dot_log, void* stream);
+                   int32_t scheme, double cfl, double t0, const pxb_re_tangent_params* params_dot, void* dt_log,
+                   void* dt_dot_log, void* stream);
 
 /* Device error word of the plan (non-finite dt or state seen by a kernel): reads it
  * (synchronising `stream`), clears it, returns PXB_OK or PXB_ERR_NONFINITE. */

@@ -111,6 +111,10 @@ class REEnsConfig(ctypes.Structure):
     ]
 
 
+class TangentParams(ctypes.Structure):
+    _fields_ = [("seds_dot", c_void_p), ("values0_dot", c_void_p)]
+
+
 class PxbError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"pyexner_b200 error {code}: {msg}")
@@ -132,9 +136,9 @@ SIGNATURES = {
     "pxb_re_run": [c_void_p, POINTER(REFields), POINTER(REFields), c_int32, c_int32, c_double, c_double, c_void_p,
                    c_void_p],
     "pxb_re_check": [c_void_p, c_void_p],
-    "pxb_re_jvp_init": [c_void_p, POINTER(REFields), POINTER(REFields), c_void_p],
+    "pxb_re_jvp_init": [c_void_p, POINTER(REFields), POINTER(REFields), c_void_p, c_void_p],
     "pxb_re_jvp_run": [c_void_p, POINTER(REFields), POINTER(REFields), c_int32, c_int32, c_double, c_double, c_void_p,
-                       c_void_p, c_void_p],
+                       c_void_p, c_void_p, c_void_p],
     "pxb_roe_plan_create": [POINTER(RoeConfig), POINTER(c_void_p)],
     "pxb_roe_plan_destroy": [c_void_p],
     "pxb_roe_cfl": [c_void_p, POINTER(RoeFields), c_double, c_void_p, c_void_p],

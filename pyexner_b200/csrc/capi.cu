@@ -255,9 +255,20 @@ struct DevHandler {
     long long* cells = nullptr;
     long long* donors = nullptr;
     double nx = 0, ny = 0, c0 = 0, c1 = 0;
-    double q = 0, vx = 0, vy = 0, hb = 0;  // ConstantOutflux, NormalFlowDepth
+    double q = 0, vx = 0, vy = 0, hb = 0;  // ConstantOutflux, NormalFlowDepth; vx, vy also ConstantInflux
     float neg_alpha = 0, zb0 = 0;          // Berthon, NormalFlowDepth
+    double c0_dot = 0, c1_dot = 0;         // tangents of c0, c1 (tangent-linear runs only)
 };
+
+// A handler constant of the arithmetic type T; dual numbers also carry its tangent.
+template <class T>
+T make_val(double v, double) {
+    return T(v);
+}
+template <>
+pxb::Dual make_val<pxb::Dual>(double v, double d) {
+    return pxb::Dual(v, d);
+}
 
 // Constants of the Berthon analytic inlet / outlet, in float32 like the reference's
 // float32 values (roeexner_berthon.py:40-52, roeexner_normalflowdepth.py:34-41):
@@ -348,6 +359,10 @@ int upload_handlers(const pxb_bc_handler* hs, int nh, long long max_index, std::
             case PXB_BC_RE_NORMALFLOWDEPTH:
                 berthon_constants(v, d);
                 break;
+            case PXB_BC_RE_CONSTANTINFLUX:  // direction of the discharge, for its tangent
+                d.vx = (float)v[1];
+                d.vy = (float)v[2];
+                break;
             case PXB_BC_RE_ZEROMOMENTUM:  // values[1] * normal (roeexner_zeromomentum.py:26-27)
                 d.c0 = (double)(float)v[1] * H.nx;
                 d.c1 = (double)(float)v[1] * H.ny;
@@ -365,6 +380,32 @@ int upload_handlers(const pxb_bc_handler* hs, int nh, long long max_index, std::
         out.push_back(d);
     }
     return PXB_OK;
+}
+
+// The float64 sediment constants of fill_sed with their tangents for a tangent of the
+// sediment matrix (same operations on the values, so the values are fill_sed's bits).
+void fill_sed_dual(pxb::SedTable<pxb::Dual>& S, const double* seds, const double* dseds, int nsed) {
+    using pxb::Dual;
+    auto at = [&](int row, int k) { return Dual(seds[row * nsed + k], dseds ? dseds[row * nsed + k] : 0.0); };
+    S = pxb::SedTable<Dual>();
+    S.n = nsed;
+    Dual por_sum = 0.0, d50f_sum = 0.0;
+    for (int k = 0; k < nsed; ++k) {
+        const Dual frac = at(0, k), d50 = at(1, k), dens = at(2, k), thc = at(5, k), por = at(6, k);
+        const Dual s = dens / Dual(1000.0);
+        const Dual np_ = pxb::hpow(d50, 1.0 / 6.0) / Dual(21.1);
+        S.s[k].np2 = np_ * np_;
+        S.s[k].sm1d = (s - Dual(1.0)) * d50;
+        S.s[k].thc = thc;
+        S.s[k].np3sg = np_ * (np_ * np_) * Dual(std::sqrt(9.81));
+        S.s[k].sm1 = s - Dual(1.0);
+        S.s[k].frac = frac;
+        por_sum = por_sum + por;
+        d50f_sum = d50f_sum + d50 * frac;
+    }
+    S.one_minus_por = Dual(1.0) - por_sum / Dual((double)nsed);
+    S.inv_one_minus_por = Dual(1.0) / (Dual(1.0) - por_sum / Dual((double)nsed));
+    S.n_p_mix = pxb::hpow(d50f_sum / Dual((double)nsed), 1.0 / 6.0) / Dual(21.1);
 }
 
 template <class T>
@@ -555,6 +596,8 @@ struct pxb_re_plan {
     pxb::DualScratch* dscr = nullptr;
     void* jvp_tmp = nullptr;
     pxb::SedTable<pxb::Dual> sedD;
+    std::vector<double> seds;  // the sediment matrix (7 x nsed), for the tangent tables
+    int nsed = 0;
     int mpm = 0;
     const uint8_t* nodata = nullptr;
     Geometry stage[8];  // by (mpm, mask, avg) variant: band geometry from its occupancy
@@ -651,23 +694,6 @@ const pxb::SedTable<double>& sed_of<double>(const pxb_re_plan* p) { return p->se
 template <>
 const pxb::SedTable<pxb::Dual>& sed_of<pxb::Dual>(const pxb_re_plan* p) { return p->sedD; }
 
-// The float64 sediment table as dual numbers with zero tangents.
-void dual_sed(pxb::SedTable<pxb::Dual>& D, const pxb::SedTable<double>& S) {
-    D.n = S.n;
-    for (int k = 0; k < PXB_MAX_SED; ++k) {
-        D.s[k].np2 = S.s[k].np2;
-        D.s[k].sm1d = S.s[k].sm1d;
-        D.s[k].thc = S.s[k].thc;
-        D.s[k].np3sg = S.s[k].np3sg;
-        D.s[k].sm1 = S.s[k].sm1;
-        D.s[k].frac = S.s[k].frac;
-        D.k_theta[k] = S.k_theta[k];
-        D.k_g1[k] = S.k_g1[k];
-    }
-    D.one_minus_por = S.one_minus_por;
-    D.n_p_mix = S.n_p_mix;
-    D.inv_one_minus_por = S.inv_one_minus_por;
-}
 
 int check_fields(const pxb_re_fields* f, bool need_g) {
     if (!f) return fail(PXB_ERR_ARG, "fields pointer is null");
@@ -755,8 +781,8 @@ int apply_handlers(const std::vector<DevHandler>& hs, void* bc_tmp, T* const f[6
         b.kind = h.kind;
         b.nx = (T)h.nx;
         b.ny = (T)h.ny;
-        b.c0 = (T)h.c0;
-        b.c1 = (T)h.c1;
+        b.c0 = make_val<T>(h.c0, h.c0_dot);
+        b.c1 = make_val<T>(h.c1, h.c1_dot);
         b.q = (T)h.q;
         b.vx = (T)h.vx;
         b.vy = (T)h.vy;
@@ -1379,6 +1405,18 @@ int check_tangent_fields(const pxb_re_fields* f, const char* what) {
     return PXB_OK;
 }
 
+// Tangents of the run's parameters: the sediment matrix (MPM constants) and the discharge
+// of ConstantInflux handlers (hu = q * values[1], hv = q * values[2]).
+void jvp_params(pxb_re_plan* P, const pxb_re_tangent_params* tp) {
+    if (P->mpm) fill_sed_dual(P->sedD, P->seds.data(), tp ? tp->seds_dot : nullptr, P->nsed);
+    for (size_t k = 0; k < P->c.handlers.size(); ++k) {
+        DevHandler& h = P->c.handlers[k];
+        const double qd = (tp && tp->values0_dot && h.kind == PXB_BC_RE_CONSTANTINFLUX) ? tp->values0_dot[k] : 0.0;
+        h.c0_dot = qd * h.vx;
+        h.c1_dot = qd * h.vy;
+    }
+}
+
 int jvp_init_impl(pxb_re_plan* P, const pxb_re_fields* f, const pxb_re_fields* fd, cudaStream_t s) {
     int st = jvp_buffers(P);
     if (st != PXB_OK) return st;
@@ -1541,7 +1579,9 @@ int pxb_re_plan_create(const pxb_re_config* cfg, pxb_re_plan** out) {
     if (cfg->mpm) {
         fill_sed(P->sedf, cfg->seds, cfg->nsed);
         fill_sed(P->sedd, cfg->seds, cfg->nsed);
-        dual_sed(P->sedD, P->sedd);
+        P->seds.assign(cfg->seds, cfg->seds + 7 * cfg->nsed);
+        P->nsed = cfg->nsed;
+        fill_sed_dual(P->sedD, P->seds.data(), nullptr, P->nsed);
     }
     const bool f64 = cfg->dtype == PXB_F64;
     for (int v = 0; v < 8; ++v) {
@@ -1638,17 +1678,22 @@ int pxb_re_run(pxb_re_plan* P, const pxb_re_fields* a, const pxb_re_fields* b, i
     return re_steps(P, a, b, nsteps, scheme, cfl, t0, dt_log, (cudaStream_t)stream);
 }
 
-int pxb_re_jvp_init(pxb_re_plan* P, const pxb_re_fields* f, const pxb_re_fields* f_dot, void* stream) {
+int pxb_re_jvp_init(pxb_re_plan* P, const pxb_re_fields* f, const pxb_re_fields* f_dot,
+                    const pxb_re_tangent_params* tp, void* stream) {
     if (!P) return fail(PXB_ERR_ARG, "null plan");
     if (P->c.dtype != PXB_F64) return fail(PXB_ERR_ARG, "the tangent-linear model runs on float64 plans");
     int st = check_tangent_fields(f, "state");
     if (st == PXB_OK) st = check_tangent_fields(f_dot, "tangent");
     if (st != PXB_OK) return st;
-    return jvp_init_impl(P, f, f_dot, (cudaStream_t)stream);
+    jvp_params(P, tp);
+    st = jvp_init_impl(P, f, f_dot, (cudaStream_t)stream);
+    jvp_params(P, nullptr);
+    return st;
 }
 
 int pxb_re_jvp_run(pxb_re_plan* P, const pxb_re_fields* a, const pxb_re_fields* a_dot, int32_t nsteps, int32_t scheme,
-                   double cfl, double t0, void* dt_log, void* dt_dot_log, void* stream) {
+                   double cfl, double t0, const pxb_re_tangent_params* tp, void* dt_log, void* dt_dot_log,
+                   void* stream) {
     if (!P) return fail(PXB_ERR_ARG, "null plan");
     if (P->c.dtype != PXB_F64) return fail(PXB_ERR_ARG, "the tangent-linear model runs on float64 plans");
     int st = check_tangent_fields(a, "state");
@@ -1657,8 +1702,11 @@ int pxb_re_jvp_run(pxb_re_plan* P, const pxb_re_fields* a, const pxb_re_fields* 
     if (nsteps < 0) return fail(PXB_ERR_ARG, "nsteps < 0");
     if (scheme != PXB_FE && scheme != PXB_SSPRK2) return fail(PXB_ERR_ARG, "scheme must be PXB_FE or PXB_SSPRK2");
     if (nsteps == 0) return PXB_OK;
-    return jvp_run_impl(P, a, a_dot, nsteps, scheme, cfl, t0, (double*)dt_log, (double*)dt_dot_log,
-                        (cudaStream_t)stream);
+    jvp_params(P, tp);
+    st = jvp_run_impl(P, a, a_dot, nsteps, scheme, cfl, t0, (double*)dt_log, (double*)dt_dot_log,
+                      (cudaStream_t)stream);
+    jvp_params(P, nullptr);
+    return st;
 }
 
 int pxb_re_check(pxb_re_plan* P, void* stream) {

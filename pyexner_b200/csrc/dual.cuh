@@ -62,6 +62,12 @@ __device__ inline Dual fabs(Dual x) { return Dual(::fabs(x.v), x.v > 0.0 ? x.d :
 __device__ inline bool d_isfinite(Dual x) { return isfinite(x.v); }
 __device__ inline Dual mul_rn(Dual a, Dual b) { return a * b; }
 
+// host side: x^y for a constant exponent (set-up tables)
+__host__ inline Dual hpow(Dual x, double y) {
+    const double p = std::pow(x.v, y);
+    return Dual(p, chain(x.d, y * std::pow(x.v, y - 1.0)));
+}
+
 // Scratch and arguments of the dual CFL reduction (tangent.cuh).
 struct DualScratch {
     unsigned long long maxbits;  // running max of the speed values' bits

@@ -14,6 +14,7 @@ from __future__ import annotations
 
 import ctypes
 
+import numpy as np
 import torch
 import torch.autograd.forward_ad as fwAD
 
@@ -31,27 +32,55 @@ def _check(state, state_dot):
         raise ValueError("state and tangent must share shape and pitch")
 
 
-def jvp_init(state, state_dot, mask, solver_config):
+def _params(solver_config, seds_dot, inflow_dot):
+    """``pxb_re_tangent_params`` for a tangent of the sediment matrix (7 x nsed, as the
+    state's ``seds``) and of the discharges of ConstantInflux handlers (dict: boundary
+    name -> tangent of its values[0])."""
+    if seds_dot is None and not inflow_dot:
+        return None, []
+    keep = []
+    p = _lib.TangentParams()
+    if seds_dot is not None:
+        sd = np.ascontiguousarray(np.asarray(seds_dot, dtype=np.float64))
+        keep.append(sd)
+        p.seds_dot = sd.ctypes.data
+    if inflow_dot:
+        names = [hd["name"] for hd in solver_config.boundaries.handlers]
+        unknown = set(inflow_dot) - set(names)
+        if unknown:
+            raise KeyError(f"no boundary named {sorted(unknown)}")
+        v = np.array([float(inflow_dot.get(n, 0.0)) for n in names], dtype=np.float64)
+        keep.append(v)
+        p.values0_dot = v.ctypes.data
+    return p, keep
+
+
+def jvp_init(state, state_dot, mask, solver_config, seds_dot=None, inflow_dot=None):
     """init_fn_roeexner and its tangent (on copies): returns (state, state_dot)."""
     _check(state, state_dot)
     s, t = state.clone(), state_dot.clone()
     plan = _re_plan(s, mask, solver_config)
-    _lib.call("pxb_re_jvp_init", plan.handle, ctypes.byref(s.c_fields()), ctypes.byref(t.c_fields()), _stream())
+    p, keep = _params(solver_config, seds_dot, inflow_dot)
+    _lib.call("pxb_re_jvp_init", plan.handle, ctypes.byref(s.c_fields()), ctypes.byref(t.c_fields()),
+              ctypes.byref(p) if p is not None else None, _stream())
     return s, t
 
 
-def jvp_run(state, state_dot, mask, solver_config, n_steps, scheme="SSPRK2", cfl=0.5, t0=0.0):
+def jvp_run(state, state_dot, mask, solver_config, n_steps, scheme="SSPRK2", cfl=0.5, t0=0.0, seds_dot=None,
+            inflow_dot=None):
     """Advance ``state`` and ``state_dot`` IN PLACE by ``n_steps`` steps; returns the dts
-    and their tangents as float64 device tensors."""
+    and their tangents as float64 device tensors.  ``seds_dot`` / ``inflow_dot``: tangents
+    of the sediment matrix and of ConstantInflux discharges (see ``_params``)."""
     _check(state, state_dot)
     plan = _re_plan(state, mask, solver_config)
+    p, keep = _params(solver_config, seds_dot, inflow_dot)
     dev = state.h.device
     dts = torch.empty(max(1, n_steps), dtype=torch.float64, device=dev)
     dts_dot = torch.empty(max(1, n_steps), dtype=torch.float64, device=dev)
     code = _lib.SSPRK2 if scheme == "SSPRK2" else _lib.FE
     _lib.call("pxb_re_jvp_run", plan.handle, ctypes.byref(state.c_fields()), ctypes.byref(state_dot.c_fields()),
-              int(n_steps), code, float(cfl), float(t0), ctypes.c_void_p(dts.data_ptr()),
-              ctypes.c_void_p(dts_dot.data_ptr()), _stream())
+              int(n_steps), code, float(cfl), float(t0), ctypes.byref(p) if p is not None else None,
+              ctypes.c_void_p(dts.data_ptr()), ctypes.c_void_p(dts_dot.data_ptr()), _stream())
     return dts[:n_steps], dts_dot[:n_steps]
 
 

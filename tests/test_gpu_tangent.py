@@ -189,3 +189,66 @@ def test_torch_forward_ad_through_the_function():
     ref = td.to_numpy()
     for f in EVOLVING:
         assert np.array_equal(got[f], ref[f]), f
+
+
+def test_parameter_tangents_grain_size_and_inflow():
+    """Tangents with respect to the grain diameter (sediment matrix row 1) and to the
+    discharge of a ConstantInflux inlet, against central differences of runs whose plans
+    are built from the perturbed parameters.  The discharge is a float32 value (as the
+    reference parses boundary values), so its difference step is 1e-3 (the float32 rounding
+    of a smaller step would dominate) and the tolerance the gradient checks' 1e-4.  A step
+    that large moves the velocity field enough to cross faces where the Exner upwind
+    direction switches (the sign of dq_b/dz_b changes where v changes sign), where the bed
+    update jumps; so for the discharge the bed itself is not differenced: h, hu, hv and G
+    are."""
+    import copy
+
+    from pyexner_b200 import BoundaryManager, RoeExnerState, create_solver_bundle, run_steps
+    from pyexner_b200.cases import seds_matrix
+    from pyexner_b200.tangent import jvp_init, jvp_run
+
+    arrs, params, X, Y = smooth_case(layout="influx_left")
+
+    def build(p):
+        bm = BoundaryManager(p, X, Y)
+        st = RoeExnerState.from_numpy(arrs, seds_matrix(p["erosion"]), torch.float64)
+        bundle = create_solver_bundle("Roe Exner")
+        cfg = bundle.config(st, None, bm, 0.1, p)
+        mask = bundle.mask_fn(st, None, bm.boundary_mask)
+        return bundle, cfg, mask, st
+
+    def with_params(d_scale, q_shift):
+        p = copy.deepcopy(params)
+        p["erosion"]["sediments"]["s1"]["diameter"] *= d_scale
+        p["boundaries"]["inlet"]["values"][0] += q_shift
+        return p
+
+    d0 = params["erosion"]["sediments"]["s1"]["diameter"]
+    # d50 moves h only through the bed: its tangent there is small, so rounding noise of the
+    # differences is relatively larger (1e-5)
+    for which, eps, tol in (("d50", 1e-6, 1e-5), ("q", 1e-3, 1e-4)):
+        bundle, cfg, mask, raw = build(params)
+        zero = raw.clone()
+        for f in raw.PLANES:
+            getattr(zero, f).zero_()
+        sd = np.zeros_like(raw.seds)
+        kw = {}
+        if which == "d50":
+            sd[1, 0] = d0  # direction: d -> d (1 + eps)
+            kw["seds_dot"] = sd
+        else:
+            kw["inflow_dot"] = {"inlet": 1.0}
+        s, td = jvp_init(raw, zero, mask, cfg, **kw)
+        jvp_run(s, td, mask, cfg, 6, "SSPRK2", 0.5, **kw)
+        outs = []
+        for sign in (1.0, -1.0):
+            pp = with_params(1.0 + sign * eps, 0.0) if which == "d50" else with_params(1.0, sign * eps)
+            b2, c2, m2, r2 = build(pp)
+            st = b2.init_fn(r2, m2, c2)
+            run_steps(st, m2, c2, "SSPRK2", 6, 0.5)
+            outs.append(st.to_numpy())
+        got = td.to_numpy()
+        for f in ("h", "hu", "hv", "z_b", "G") if which == "d50" else ("h", "hu", "hv", "G"):
+            fd = (outs[0][f] - outs[1][f]) / (2 * eps)
+            assert np.max(np.abs(fd)) > 0, (which, f)
+            assert rel_err(got[f], fd) <= tol, (which, f, rel_err(got[f], fd))
