@@ -204,6 +204,21 @@ int pxb_re_jvp_run(pxb_re_plan* plan, const pxb_re_fields* a, const pxb_re_field
                    int32_t scheme, double cfl, double t0, const pxb_re_tangent_params* params_dot, void* dt_log,
                    void* dt_dot_log, void* stream);
 
+/* Reverse mode (adjoint), float64 plans.  No counterpart in the reference's code (JAX
+ * would give it with jax.vjp over a fixed-length loop).  pxb_re_vjp_run: `a0` is the state
+ * after init (not modified); `abar` holds the adjoint of the state after nsteps steps
+ * (dJ/du for h, hu, hv, z_b, G) and receives the adjoint of a0.  The steps are redone
+ * forward with a checkpoint every `checkpoint_every` steps (0: 32) and undone segment by
+ * segment: each stage backwards (handlers, Exner update, grass factor, corrections, hydro
+ * update), with local Jacobians of the faces from multi-tangent dual numbers, and the
+ * dependence of dt on the state through the fastest face.  pxb_re_vjp_init: `f` is the
+ * state BEFORE init; `fbar` (in: adjoint after init, out: before) goes back through the
+ * handlers and the grass factor.  Handlers of every kind but ConstantOutflux.  Allocates
+ * its checkpoints for the call; synchronises `stream`. */
+int pxb_re_vjp_init(pxb_re_plan* plan, const pxb_re_fields* f, const pxb_re_fields* fbar, void* stream);
+int pxb_re_vjp_run(pxb_re_plan* plan, const pxb_re_fields* a0, int32_t nsteps, int32_t scheme, double cfl, double t0,
+                   int32_t checkpoint_every, const pxb_re_fields* abar, void* stream);
+
 /* Device error word of the plan (non-finite dt or state seen by a kernel): reads it
  * (synchronising `stream`), clears it, returns PXB_OK or PXB_ERR_NONFINITE. */
 int pxb_re_check(pxb_re_plan* plan, void* stream);

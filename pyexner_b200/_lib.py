@@ -136,6 +136,9 @@ SIGNATURES = {
     "pxb_re_run": [c_void_p, POINTER(REFields), POINTER(REFields), c_int32, c_int32, c_double, c_double, c_void_p,
                    c_void_p],
     "pxb_re_check": [c_void_p, c_void_p],
+    "pxb_re_vjp_init": [c_void_p, POINTER(REFields), POINTER(REFields), c_void_p],
+    "pxb_re_vjp_run": [c_void_p, POINTER(REFields), c_int32, c_int32, c_double, c_double, c_int32, POINTER(REFields),
+                       c_void_p],
     "pxb_re_jvp_init": [c_void_p, POINTER(REFields), POINTER(REFields), c_void_p, c_void_p],
     "pxb_re_jvp_run": [c_void_p, POINTER(REFields), POINTER(REFields), c_int32, c_int32, c_double, c_double, c_void_p,
                        c_void_p, c_void_p, c_void_p],

@@ -27,6 +27,7 @@ UNITS = [
     ("kernels_f64.cu", ["-fmad=false"]),
     ("setup_f64.cu", ["-fmad=false"]),
     ("kernels_dual.cu", ["-fmad=false"]),
+    ("kernels_adj.cu", ["-fmad=false"]),
     ("capi.cu", []),
     ("noalloc.cu", []),
 ]

@@ -21,6 +21,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "adjoint_args.cuh"
 #include "pxb_launch.h"
 
 namespace {
@@ -1480,6 +1481,381 @@ int jvp_run_impl(pxb_re_plan* P, const pxb_re_fields* a, const pxb_re_fields* ad
     return jvp_unpack(P, cur, a, ad, s);
 }
 
+// ------------------------------------------------------------------ reverse mode
+// State planes carried by the adjoint: h, hu, hv, z_b, G (z, n_b static; n has no effect).
+struct Planes5 {
+    double* p[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+};
+
+Planes5 planes_of(double* base, size_t plane, int k) {
+    Planes5 q;
+    for (int f = 0; f < 5; ++f) q.p[f] = base + ((size_t)k * 5 + f) * plane;
+    return q;
+}
+
+pxb_re_fields fields_of(const Planes5& q, const pxb_re_fields* statics) {
+    pxb_re_fields f{};
+    f.h = q.p[0];
+    f.hu = q.p[1];
+    f.hv = q.p[2];
+    f.z_b = q.p[3];
+    f.G = q.p[4];
+    f.z = statics->z;
+    f.n_b = statics->n_b;
+    f.n = nullptr;
+    return f;
+}
+
+int copy5(PlanCommon& C, const Planes5& dst, const Planes5& src, cudaStream_t s) {
+    for (int f = 0; f < 5; ++f)
+        PXB_CUDA(cudaMemcpyAsync(dst.p[f], src.p[f], sizeof(double) * (size_t)C.ny * C.pitch, cudaMemcpyDeviceToDevice, s));
+    return PXB_OK;
+}
+
+int zero5(PlanCommon& C, const Planes5& q, cudaStream_t s) {
+    for (int f = 0; f < 5; ++f) PXB_CUDA(cudaMemsetAsync(q.p[f], 0, sizeof(double) * (size_t)C.ny * C.pitch, s));
+    return PXB_OK;
+}
+
+// Handlers backwards (last to first) on adjoint planes (slots h, hu, hv, z_b, -, G).
+int adj_handlers(PlanCommon& C, double* const f[6], double* tmp, cudaStream_t s) {
+    for (size_t q = C.handlers.size(); q-- > 0;) {
+        const DevHandler& h = C.handlers[q];
+        pxb::AdjBcArgs b{};
+        for (int k = 0; k < 6; ++k) b.f[k] = f[k];
+        b.cells = h.cells;
+        b.donors = h.donors;
+        b.count = h.count;
+        b.kind = h.kind;
+        b.nx = h.nx;
+        b.ny = h.ny;
+        b.c0 = h.c0;
+        b.c1 = h.c1;
+        b.tmp = tmp;
+        PXB_CUDA(pxb::launch_adj_bc(b, s));
+    }
+    return PXB_OK;
+}
+
+struct AdjWork {
+    double* base = nullptr;  // all planes
+    size_t plane = 0;
+    int nck = 0, K = 0;
+    Planes5 u1, aS, aT, aCur, aNext, aU1;
+    double* h1 = nullptr;
+    double* gscr = nullptr;  // 7 planes for the general stage
+    double* dev = nullptr;   // dt, dtbar, times (checkpoints then segment)
+    unsigned long long* maxbits = nullptr;
+    unsigned int* nties = nullptr;
+    double* bctmp = nullptr;
+    Planes5 ck(int k) const { return planes_of(base, plane, k); }                  // checkpoint k
+    Planes5 seg(int k) const { return planes_of(base, plane, nck + k); }           // segment state k
+    void release() {
+        cudaFree(base);
+        cudaFree(dev);
+        cudaFree(maxbits);
+        cudaFree(bctmp);
+        base = dev = nullptr;
+        maxbits = nullptr;
+        bctmp = nullptr;
+    }
+};
+
+// The stage input's adjoint += the reverse of one stage, given the adjoint of its output in
+// W.aS (overwritten).  The stage internals are recomputed from the input first.
+int adj_stage(pxb_re_plan* P, AdjWork& W, const pxb_re_fields* in, const Planes5& aIn, const double* dt,
+              const double* tptr, cudaStream_t s) {
+    const size_t plane = W.plane;
+    double* S = W.gscr;
+    // forward recompute: hydro, corrections, handlers 1, grass (as re_general_impl)
+    pxb::GenArgs<double> g{};
+    g.ny = P->c.ny;
+    g.nx = P->c.nx;
+    g.pitch = P->c.pitch;
+    g.dx = P->c.dx;
+    g.h = (const double*)in->h;
+    g.hu = (const double*)in->hu;
+    g.hv = (const double*)in->hv;
+    g.zb = (const double*)in->z_b;
+    g.z = (const double*)in->z;
+    g.nb = (const double*)in->n_b;
+    g.G = (const double*)in->G;
+    g.n = nullptr;
+    g.sh = S;
+    g.shu = S + plane;
+    g.shv = S + 2 * plane;
+    g.szb = S + 3 * plane;
+    g.sG = S + 4 * plane;
+    g.sn = S + 5 * plane;
+    g.szb2 = S + 6 * plane;
+    g.nodata = P->nodata;
+    g.dt = dt;
+    g.sed = P->sedd;
+    g.mpm = P->mpm;
+    g.err = &P->c.scr->err;
+    PXB_CUDA(pxb::launch_re_general<double>(g, pxb::GEN_HYDRO, s));
+    PXB_CUDA(pxb::launch_re_general<double>(g, pxb::GEN_CORR, s));
+    PXB_CUDA(cudaMemcpyAsync(W.h1, g.sh, sizeof(double) * plane, cudaMemcpyDeviceToDevice, s));
+    double* const f1[6] = {g.sh, g.shu, g.shv, g.szb, g.sn, g.sG};
+    int st = apply_handlers<double>(P->c.handlers, P->c.bc_tmp, f1, tptr, 0.0, s);
+    if (st != PXB_OK) return st;
+    PXB_CUDA(pxb::launch_re_general<double>(g, pxb::GEN_GRASS, s));
+    // backwards
+    pxb::AdjArgs a{};
+    a.ny = P->c.ny;
+    a.nx = P->c.nx;
+    a.pitch = P->c.pitch;
+    a.dx = P->c.dx;
+    a.h = g.h;
+    a.hu = g.hu;
+    a.hv = g.hv;
+    a.zb = g.zb;
+    a.z = g.z;
+    a.nb = g.nb;
+    a.G = g.G;
+    a.h1 = W.h1;
+    a.sh = g.sh;
+    a.shu = g.shu;
+    a.shv = g.shv;
+    a.szb = g.szb;
+    a.sG = g.sG;
+    a.nodata = P->nodata;
+    a.dt = dt;
+    a.sed = P->sedd;
+    a.mpm = P->mpm;
+    a.Sh = W.aS.p[0];
+    a.Shu = W.aS.p[1];
+    a.Shv = W.aS.p[2];
+    a.Szb = W.aS.p[3];
+    a.SG = W.aS.p[4];
+    a.Th = W.aT.p[0];
+    a.Thu = W.aT.p[1];
+    a.Thv = W.aT.p[2];
+    a.Tzb = W.aT.p[3];
+    a.TG = W.aT.p[4];
+    a.Ih = aIn.p[0];
+    a.Ihu = aIn.p[1];
+    a.Ihv = aIn.p[2];
+    a.Izb = aIn.p[3];
+    a.IG = aIn.p[4];
+    a.dtbar = W.dev + 1;
+    double* const fS[6] = {W.aS.p[0], W.aS.p[1], W.aS.p[2], W.aS.p[3], nullptr, W.aS.p[4]};
+    st = adj_handlers(P->c, fS, W.bctmp, s);  // handlers 2
+    if (st != PXB_OK) return st;
+    PXB_CUDA(pxb::launch_adj_stage(a, 0, s));  // Exner
+    PXB_CUDA(pxb::launch_adj_stage(a, 1, s));  // grass
+    double* const fT[6] = {W.aT.p[0], W.aT.p[1], W.aT.p[2], W.aT.p[3], nullptr, W.aT.p[4]};
+    st = adj_handlers(P->c, fT, W.bctmp, s);  // handlers 1
+    if (st != PXB_OK) return st;
+    PXB_CUDA(pxb::launch_adj_stage(a, 2, s));  // corrections
+    PXB_CUDA(pxb::launch_adj_stage(a, 3, s));  // hydro
+    return PXB_OK;
+}
+
+// One forward stage on the general kernels (float64) into `out`.
+int adj_fwd_stage(pxb_re_plan* P, AdjWork& W, const pxb_re_fields* in, const pxb_re_fields* out,
+                  const pxb_re_fields* avg, const double* dt, const double* tptr, cudaStream_t s) {
+    return re_general_impl<double>(P, in, out, avg, dt, tptr, 0.0, s, W.gscr, P->c.bc_tmp);
+}
+
+int adj_step_fwd(pxb_re_plan* P, AdjWork& W, const Planes5& u, const Planes5& next, int scheme,
+                 const pxb_re_fields* statics, double cfl, cudaStream_t s) {
+    double* dt = W.dev;
+    const pxb_re_fields F = fields_of(u, statics), U1 = fields_of(W.u1, statics), N = fields_of(next, statics);
+    int st = re_cfl_impl<double>(P, &F, cfl, dt, nullptr, s);
+    if (st != PXB_OK) return st;
+    const double* tptr = &P->c.scr->t_step;
+    st = adj_fwd_stage(P, W, &F, &U1, nullptr, dt, tptr, s);
+    if (st != PXB_OK) return st;
+    if (scheme == PXB_SSPRK2) return adj_fwd_stage(P, W, &U1, &N, &F, dt, tptr, s);
+    return copy5(P->c, next, W.u1, s);
+}
+
+int vjp_run_impl(pxb_re_plan* P, const pxb_re_fields* a0, int nsteps, int scheme, double cfl, double t0, int every,
+                 const pxb_re_fields* abar, cudaStream_t s) {
+    for (auto& h : P->c.handlers)
+        if (h.kind == PXB_BC_RE_CONSTANTOUTFLUX)
+            return fail(PXB_ERR_UNSUPPORTED, "the reverse mode does not cover ConstantOutflux handlers (nonlinear)");
+    AdjWork W;
+    W.K = every > 0 ? every : 32;
+    W.nck = (nsteps + W.K - 1) / W.K;
+    W.plane = (size_t)P->c.ny * (size_t)P->c.pitch;
+    // checkpoints, segment states (K + 1), u1, aS, aT, aCur, aNext, aU1 (5 planes each), h1, 7 scratch
+    const size_t nplanes = (size_t)5 * (W.nck + W.K + 1 + 6) + 1 + 7;
+    int maxcount = 1;
+    for (auto& h : P->c.handlers) maxcount = std::max(maxcount, h.count);
+    auto bail = [&](int code) {
+        cudaStreamSynchronize(s);
+        W.release();
+        return code;
+    };
+    if (cudaMalloc(&W.base, sizeof(double) * nplanes * W.plane) != cudaSuccess ||
+        cudaMalloc(&W.dev, sizeof(double) * (2 + W.nck + W.K)) != cudaSuccess ||
+        cudaMalloc(&W.maxbits, 16) != cudaSuccess ||
+        cudaMalloc(&W.bctmp, sizeof(double) * 6 * (size_t)maxcount) != cudaSuccess)
+        return bail(fail(PXB_ERR_CUDA, "reverse-mode buffers"));
+    W.nties = (unsigned int*)(W.maxbits + 1);
+    const int o = W.nck + W.K + 1;
+    W.u1 = planes_of(W.base, W.plane, o);
+    W.aS = planes_of(W.base, W.plane, o + 1);
+    W.aT = planes_of(W.base, W.plane, o + 2);
+    W.aCur = planes_of(W.base, W.plane, o + 3);
+    W.aNext = planes_of(W.base, W.plane, o + 4);
+    W.aU1 = planes_of(W.base, W.plane, o + 5);
+    W.h1 = W.base + (size_t)5 * (o + 6) * W.plane;
+    W.gscr = W.h1 + W.plane;
+    double* tck = W.dev + 2;
+    double* tseg = tck + W.nck;
+    Planes5 A0;
+    A0.p[0] = (double*)a0->h;
+    A0.p[1] = (double*)a0->hu;
+    A0.p[2] = (double*)a0->hv;
+    A0.p[3] = (double*)a0->z_b;
+    A0.p[4] = (double*)a0->G;
+    int st = PXB_OK;
+    auto chk = [&](int r) {
+        if (st == PXB_OK) st = r;
+        return st == PXB_OK;
+    };
+    // forward sweep with checkpoints
+    chk(copy5(P->c, W.ck(0), A0, s));
+    if (st == PXB_OK && pxb::launch_set_time<double>(P->c.scr, t0, s) != cudaSuccess) st = fail(PXB_ERR_CUDA, "time");
+    for (int n = 0; n < nsteps && st == PXB_OK; ++n) {
+        const int k = n / W.K;
+        if (n % W.K == 0) {
+            if (n > 0) chk(copy5(P->c, W.ck(k), W.seg(0), s));
+            if (cudaMemcpyAsync(tck + k, &P->c.scr->t_next, 8, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+                st = fail(PXB_ERR_CUDA, "checkpoint time");
+            if (n == 0) chk(copy5(P->c, W.seg(0), A0, s));
+        }
+        if (st == PXB_OK) chk(adj_step_fwd(P, W, W.seg(0), W.seg(0), scheme, a0, cfl, s));
+    }
+    // backward sweep
+    const pxb_re_fields* statics = a0;
+    Planes5 AB;
+    AB.p[0] = (double*)abar->h;
+    AB.p[1] = (double*)abar->hu;
+    AB.p[2] = (double*)abar->hv;
+    AB.p[3] = (double*)abar->z_b;
+    AB.p[4] = (double*)abar->G;
+    if (st == PXB_OK) chk(copy5(P->c, W.aNext, AB, s));
+    for (int k = W.nck - 1; k >= 0 && st == PXB_OK; --k) {
+        const int n0 = k * W.K, n1 = std::min(nsteps, n0 + W.K);
+        chk(copy5(P->c, W.seg(0), W.ck(k), s));
+        if (st == PXB_OK && cudaMemcpyAsync(&P->c.scr->t_next, tck + k, 8, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+            st = fail(PXB_ERR_CUDA, "segment time");
+        for (int j = 0; j < n1 - n0 - 1 && st == PXB_OK; ++j) {
+            if (cudaMemcpyAsync(tseg + j, &P->c.scr->t_next, 8, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+                st = fail(PXB_ERR_CUDA, "step time");
+            else chk(adj_step_fwd(P, W, W.seg(j), W.seg(j + 1), scheme, statics, cfl, s));
+        }
+        if (st == PXB_OK && n1 - n0 - 1 >= 0 &&
+            cudaMemcpyAsync(tseg + (n1 - n0 - 1), &P->c.scr->t_next, 8, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+            st = fail(PXB_ERR_CUDA, "step time");
+        for (int j = n1 - n0 - 1; j >= 0 && st == PXB_OK; --j) {
+            const Planes5 u = W.seg(j);
+            const pxb_re_fields F = fields_of(u, statics), U1 = fields_of(W.u1, statics);
+            double* dt = W.dev;
+            // the step's time and dt again (the CFL kernel moves t_next into t_step)
+            if (cudaMemcpyAsync(&P->c.scr->t_next, tseg + j, 8, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+                cudaMemsetAsync(W.dev + 1, 0, sizeof(double), s) != cudaSuccess) {
+                st = fail(PXB_ERR_CUDA, "step state");
+                break;
+            }
+            if (!chk(re_cfl_impl<double>(P, &F, cfl, dt, nullptr, s))) break;
+            const double* tptr = &P->c.scr->t_step;
+            if (!chk(zero5(P->c, W.aCur, s))) break;
+            if (scheme == PXB_SSPRK2) {
+                const double* o5[5] = {W.aNext.p[0], W.aNext.p[1], W.aNext.p[2], W.aNext.p[3], W.aNext.p[4]};
+                if (!chk(adj_fwd_stage(P, W, &F, &U1, nullptr, dt, tptr, s))) break;
+                if (pxb::launch_adj_store(P->c.ny, P->c.nx, P->c.pitch, 0.5, o5, W.aS.p, W.aCur.p, s) != cudaSuccess) {
+                    st = fail(PXB_ERR_CUDA, "adjoint store");
+                    break;
+                }
+                if (!chk(zero5(P->c, W.aU1, s))) break;
+                if (!chk(adj_stage(P, W, &U1, W.aU1, dt, tptr, s))) break;
+                const double* o1[5] = {W.aU1.p[0], W.aU1.p[1], W.aU1.p[2], W.aU1.p[3], W.aU1.p[4]};
+                if (pxb::launch_adj_store(P->c.ny, P->c.nx, P->c.pitch, 1.0, o1, W.aS.p, nullptr, s) != cudaSuccess) {
+                    st = fail(PXB_ERR_CUDA, "adjoint store");
+                    break;
+                }
+                if (!chk(adj_stage(P, W, &F, W.aCur, dt, tptr, s))) break;
+            } else {
+                const double* o5[5] = {W.aNext.p[0], W.aNext.p[1], W.aNext.p[2], W.aNext.p[3], W.aNext.p[4]};
+                if (pxb::launch_adj_store(P->c.ny, P->c.nx, P->c.pitch, 1.0, o5, W.aS.p, nullptr, s) != cudaSuccess) {
+                    st = fail(PXB_ERR_CUDA, "adjoint store");
+                    break;
+                }
+                if (!chk(adj_stage(P, W, &F, W.aCur, dt, tptr, s))) break;
+            }
+            // dt depends on the step's input through the fastest face
+            pxb::AdjCflArgs c{};
+            c.ny = P->c.ny;
+            c.nx = P->c.nx;
+            c.pitch = P->c.pitch;
+            c.h = (const double*)F.h;
+            c.hu = (const double*)F.hu;
+            c.hv = (const double*)F.hv;
+            c.G = (const double*)F.G;
+            c.nodata = P->nodata;
+            c.dx = P->c.dx;
+            c.cfl = cfl;
+            c.floor_dt = pxb::DT_FLOOR;
+            c.maxbits = W.maxbits;
+            c.nties = W.nties;
+            c.dtbar = W.dev + 1;
+            c.Ah = W.aCur.p[0];
+            c.Ahu = W.aCur.p[1];
+            c.Ahv = W.aCur.p[2];
+            c.AG = W.aCur.p[4];
+            if (cudaMemsetAsync(W.maxbits, 0, 16, s) != cudaSuccess || pxb::launch_adj_cfl(c, s) != cudaSuccess) {
+                st = fail(PXB_ERR_CUDA, "adjoint of dt");
+                break;
+            }
+            std::swap(W.aCur, W.aNext);
+        }
+    }
+    if (st == PXB_OK) chk(copy5(P->c, AB, W.aNext, s));
+    cudaStreamSynchronize(s);
+    W.release();
+    return st;
+}
+
+// init_fn_roeexner backwards: handlers (t = 0), then the grass factor from the raw state.
+int vjp_init_impl(pxb_re_plan* P, const pxb_re_fields* f, const pxb_re_fields* fbar, cudaStream_t s) {
+    for (auto& h : P->c.handlers)
+        if (h.kind == PXB_BC_RE_CONSTANTOUTFLUX)
+            return fail(PXB_ERR_UNSUPPORTED, "the reverse mode does not cover ConstantOutflux handlers (nonlinear)");
+    int maxcount = 1;
+    for (auto& h : P->c.handlers) maxcount = std::max(maxcount, h.count);
+    double* tmp = nullptr;
+    PXB_CUDA(cudaMalloc(&tmp, sizeof(double) * 6 * (size_t)maxcount));
+    double* const fb[6] = {(double*)fbar->h, (double*)fbar->hu, (double*)fbar->hv, (double*)fbar->z_b, nullptr,
+                           (double*)fbar->G};
+    int st = adj_handlers(P->c, fb, tmp, s);
+    if (st == PXB_OK) {
+        pxb::AdjArgs a{};
+        a.ny = P->c.ny;
+        a.nx = P->c.nx;
+        a.pitch = P->c.pitch;
+        a.dx = P->c.dx;
+        a.sh = (const double*)f->h;
+        a.shu = (const double*)f->hu;
+        a.shv = (const double*)f->hv;
+        a.nodata = P->nodata;
+        a.sed = P->sedd;
+        a.mpm = P->mpm;
+        a.Th = fb[0];
+        a.Thu = fb[1];
+        a.Thv = fb[2];
+        a.TG = fb[5];
+        if (pxb::launch_adj_stage(a, 1, s) != cudaSuccess) st = fail(PXB_ERR_CUDA, "adjoint of the grass factor");
+    }
+    cudaStreamSynchronize(s);
+    cudaFree(tmp);
+    return st;
+}
+
 }  // namespace
 
 // ===================================================================== C entry points
@@ -1707,6 +2083,29 @@ int pxb_re_jvp_run(pxb_re_plan* P, const pxb_re_fields* a, const pxb_re_fields* 
                       (cudaStream_t)stream);
     jvp_params(P, nullptr);
     return st;
+}
+
+int pxb_re_vjp_init(pxb_re_plan* P, const pxb_re_fields* f, const pxb_re_fields* fbar, void* stream) {
+    if (!P) return fail(PXB_ERR_ARG, "null plan");
+    if (P->c.dtype != PXB_F64) return fail(PXB_ERR_ARG, "the reverse mode runs on float64 plans");
+    if (!f || !f->h || !f->hu || !f->hv) return fail(PXB_ERR_ARG, "state: h, hu and hv must be set");
+    if (!fbar || !fbar->h || !fbar->hu || !fbar->hv || !fbar->z_b || !fbar->G)
+        return fail(PXB_ERR_ARG, "adjoint: h, hu, hv, z_b and G must be set");
+    return vjp_init_impl(P, f, fbar, (cudaStream_t)stream);
+}
+
+int pxb_re_vjp_run(pxb_re_plan* P, const pxb_re_fields* a0, int32_t nsteps, int32_t scheme, double cfl, double t0,
+                   int32_t checkpoint_every, const pxb_re_fields* abar, void* stream) {
+    if (!P) return fail(PXB_ERR_ARG, "null plan");
+    if (P->c.dtype != PXB_F64) return fail(PXB_ERR_ARG, "the reverse mode runs on float64 plans");
+    if (!a0 || !a0->h || !a0->hu || !a0->hv || !a0->z || !a0->z_b || !a0->n_b || !a0->G)
+        return fail(PXB_ERR_ARG, "state: h, hu, hv, z, z_b, n_b and G must be set");
+    if (!abar || !abar->h || !abar->hu || !abar->hv || !abar->z_b || !abar->G)
+        return fail(PXB_ERR_ARG, "adjoint: h, hu, hv, z_b and G must be set");
+    if (nsteps < 0) return fail(PXB_ERR_ARG, "nsteps < 0");
+    if (scheme != PXB_FE && scheme != PXB_SSPRK2) return fail(PXB_ERR_ARG, "scheme must be PXB_FE or PXB_SSPRK2");
+    if (nsteps == 0) return PXB_OK;
+    return vjp_run_impl(P, a0, nsteps, scheme, cfl, t0, checkpoint_every, abar, (cudaStream_t)stream);
 }
 
 int pxb_re_check(pxb_re_plan* P, void* stream) {

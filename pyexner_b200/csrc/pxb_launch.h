@@ -43,6 +43,16 @@ cudaError_t launch_re_general(const GenArgs<T>& a, int phase, cudaStream_t s);
 template <class T>
 cudaError_t launch_set_time(CflScratch* scr, double t0, cudaStream_t s);
 
+// Reverse mode (kernels_adj.cu); the argument structs are in adjoint_args.cuh.
+struct AdjArgs;
+struct AdjBcArgs;
+struct AdjCflArgs;
+cudaError_t launch_adj_store(int ny, int nx, long long pitch, double scale, const double* const o[5], double* const S[5],
+                             double* const A[5], cudaStream_t s);
+cudaError_t launch_adj_stage(const AdjArgs& a, int phase, cudaStream_t s);
+cudaError_t launch_adj_bc(const AdjBcArgs& a, cudaStream_t s);
+cudaError_t launch_adj_cfl(const AdjCflArgs& a, cudaStream_t s);
+
 // Tangent-linear model (kernels_dual.cu).
 cudaError_t launch_dual_cfl(const DualCflArgs& a, cudaStream_t s);
 cudaError_t launch_dual_pack(int ny, int nx, long long pitch, const double* v, const double* t, Dual* out,

@@ -138,3 +138,34 @@ class RoeExnerSteps(torch.autograd.Function):
 
 
 __all__ = ["jvp_init", "jvp_run", "RoeExnerSteps", "StepsSpec", "fwAD"]
+
+
+# ------------------------------------------------------------------ reverse mode
+def _adj_fields(abar):
+    return abar.c_fields()
+
+
+def vjp_run(state0, abar, mask, solver_config, n_steps, scheme="SSPRK2", cfl=0.5, t0=0.0, checkpoint_every=32):
+    """Reverse mode of ``n_steps`` fixed steps from ``state0`` (the state after init, not
+    modified): ``abar`` (a RoeExnerState whose h, hu, hv, z_b, G hold dJ/du of the final
+    state) is overwritten IN PLACE with dJ/du of ``state0``.  The run is redone forward
+    with a checkpoint every ``checkpoint_every`` steps and undone segment by segment."""
+    _check(state0, abar)
+    plan = _re_plan(state0, mask, solver_config)
+    _lib.call("pxb_re_vjp_run", plan.handle, ctypes.byref(state0.c_fields()), int(n_steps),
+              _lib.SSPRK2 if scheme == "SSPRK2" else _lib.FE, float(cfl), float(t0), int(checkpoint_every),
+              ctypes.byref(_adj_fields(abar)), _stream())
+    return abar
+
+
+def vjp_init(state_raw, abar, mask, solver_config):
+    """Reverse mode of init_fn_roeexner: ``abar`` (adjoint of the state after init) is
+    overwritten IN PLACE with the adjoint of ``state_raw`` (the state before init)."""
+    _check(state_raw, abar)
+    plan = _re_plan(state_raw, mask, solver_config)
+    _lib.call("pxb_re_vjp_init", plan.handle, ctypes.byref(state_raw.c_fields()), ctypes.byref(_adj_fields(abar)),
+              _stream())
+    return abar
+
+
+__all__ += ["vjp_run", "vjp_init"]

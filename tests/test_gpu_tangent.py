@@ -252,3 +252,86 @@ def test_parameter_tangents_grain_size_and_inflow():
             fd = (outs[0][f] - outs[1][f]) / (2 * eps)
             assert np.max(np.abs(fd)) > 0, (which, f)
             assert rel_err(got[f], fd) <= tol, (which, f, rel_err(got[f], fd))
+
+
+# ------------------------------------------------------------------ reverse mode
+def inner(a, b, fields=("h", "hu", "hv", "z_b", "G")):
+    A, B = a.to_numpy(), b.to_numpy()
+    return float(sum(np.sum(A[f] * B[f]) for f in fields))
+
+
+def random_adjoint(st, rng, fields=("h", "hu", "hv", "z_b", "G")):
+    t = st.clone()
+    for f in st.PLANES:
+        getattr(t, f).zero_()
+    for f in fields:
+        getattr(t, f).copy_(torch.from_numpy(rng.standard_normal(st.shape)))
+    return t
+
+
+@pytest.mark.parametrize("scheme,layout,every", [("SSPRK2", "trans_x_refl_y", 32), ("SSPRK2", "influx_left", 3),
+                                                 ("FE", "refl_all", 4), ("SSPRK2", "l_domain", 5)])
+def test_adjoint_is_the_transpose_of_the_tangent(scheme, layout, every):
+    """<abar_0, du_0> == <abar_N, J du_0>: the reverse mode (checkpointed, segments of
+    `every` steps) against the tangent-linear run of the same 8 steps; both differentiate
+    the same discrete map with the same branch choices, so they agree to rounding."""
+    from pyexner_b200.tangent import jvp_run, vjp_run
+
+    args = smooth_case(layout=layout)
+    if layout == "l_domain":
+        args[0]["z"][:6, -6:] = np.nan
+    bundle, cfg, mask, st = setup(*args)
+    rng = np.random.default_rng(17)
+    du = tangent_state(st, rng, ("h", "hu", "hv", "z_b"))
+    s, td = st.clone(), du.clone()
+    jvp_run(s, td, mask, cfg, 8, scheme, 0.5)
+    abar = random_adjoint(st, rng)
+    rhs = inner(abar, td)
+    a0 = vjp_run(st, abar.clone(), mask, cfg, 8, scheme, 0.5, checkpoint_every=every)
+    lhs = inner(a0, du, ("h", "hu", "hv", "z_b"))
+    assert abs(lhs - rhs) <= 1e-9 * max(abs(rhs), 1e-30), (lhs, rhs)
+
+
+def test_bed_gradient_against_central_differences():
+    """Gradient of J = sum (z + z_b - target)^2 after 10 SSPRK2 steps with respect to the
+    bed of 12 random cells (through init), against central differences (eps 1e-6)."""
+    from pyexner_b200 import BoundaryManager, RoeExnerState, create_solver_bundle, run_steps
+    from pyexner_b200.cases import seds_matrix
+    from pyexner_b200.tangent import vjp_init, vjp_run
+
+    arrs, params, X, Y = smooth_case()
+    bm = BoundaryManager(params, X, Y)
+    raw = RoeExnerState.from_numpy(arrs, seds_matrix(params["erosion"]), torch.float64)
+    bundle = create_solver_bundle("Roe Exner")
+    cfg = bundle.config(raw, None, bm, 0.1, params)
+    mask = bundle.mask_fn(raw, None, bm.boundary_mask)
+    rng = np.random.default_rng(23)
+    target = (arrs["z"] + arrs["z_b"]) + 0.001 * rng.standard_normal(arrs["h"].shape)
+
+    def objective(st0_raw):
+        st = bundle.init_fn(st0_raw, mask, cfg)
+        run_steps(st, mask, cfg, "SSPRK2", 10, 0.5)
+        s = st.to_numpy()
+        return float(np.sum((s["z"] + s["z_b"] - target) ** 2)), st
+
+    J0, stN = objective(raw)
+    s = stN.to_numpy()
+    abar = raw.clone()
+    for f in raw.PLANES:
+        getattr(abar, f).zero_()
+    abar.z_b.copy_(torch.from_numpy(2 * (s["z"] + s["z_b"] - target)))
+    st0 = bundle.init_fn(raw, mask, cfg)
+    vjp_run(st0, abar, mask, cfg, 10, "SSPRK2", 0.5, checkpoint_every=4)
+    vjp_init(raw, abar, mask, cfg)
+    grad = abar.to_numpy()["z_b"]
+    ny, nx = raw.shape
+    cells = [(int(rng.integers(1, ny - 1)), int(rng.integers(1, nx - 1))) for _ in range(12)]
+    eps = 1e-6
+    for (r, c) in cells:
+        vals = []
+        for sign in (1.0, -1.0):
+            p = raw.clone()
+            p.z_b[r, c] += sign * eps
+            vals.append(objective(p)[0])
+        fd = (vals[0] - vals[1]) / (2 * eps)
+        assert abs(grad[r, c] - fd) <= 1e-5 * max(abs(fd), 1e-8), ((r, c), grad[r, c], fd)
