@@ -105,12 +105,16 @@ def _state_from(planes, seds):
 
 class RoeExnerSteps(torch.autograd.Function):
     """``spec.n_steps`` fixed steps of the float64 Roe-Exner bundle as a differentiable
-    function of the eight state planes (h, hu, hv, z, z_b, n, n_b, G), forward mode only:
+    function of the eight state planes (h, hu, hv, z, z_b, n, n_b, G).  Forward mode runs
+    the tangent-linear kernels:
 
         with fwAD.dual_level():
             planes = [fwAD.make_dual(p, t) for p, t in zip(planes, tangents)]
             out = RoeExnerSteps.apply(spec, *planes)
             tangents_out = [fwAD.unpack_dual(o).tangent for o in out]
+
+    and reverse mode (``loss.backward()``, ``torch.autograd.grad``) the adjoint kernels,
+    which give gradients for h, hu, hv, z_b and G (z, n and n_b are held constant).
     """
 
     @staticmethod
@@ -119,6 +123,7 @@ class RoeExnerSteps(torch.autograd.Function):
 
         ctx.spec = spec
         ctx.save_for_forward(*planes)
+        ctx.save_for_backward(*planes)
         st = _state_from(planes, spec.seds)
         run_steps(st, spec.mask, spec.cfg, spec.scheme, spec.n_steps, spec.cfl, log_dt=False)
         return tuple(getattr(st, f).clone() for f in RoeExnerState.PLANES)
@@ -134,7 +139,13 @@ class RoeExnerSteps(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, *grads):
-        raise NotImplementedError("RoeExnerSteps provides forward-mode derivatives only")
+        spec = ctx.spec
+        planes = ctx.saved_tensors
+        st = _state_from(planes, spec.seds)
+        abar = _state_from([g if g is not None else torch.zeros_like(p) for g, p in zip(grads, planes)], spec.seds)
+        vjp_run(st, abar, spec.mask, spec.cfg, spec.n_steps, spec.scheme, spec.cfl)
+        carried = ("h", "hu", "hv", "z_b", "G")
+        return (None,) + tuple(getattr(abar, f).clone() if f in carried else None for f in RoeExnerState.PLANES)
 
 
 __all__ = ["jvp_init", "jvp_run", "RoeExnerSteps", "StepsSpec", "fwAD"]

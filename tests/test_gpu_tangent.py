@@ -335,3 +335,28 @@ def test_bed_gradient_against_central_differences():
             vals.append(objective(p)[0])
         fd = (vals[0] - vals[1]) / (2 * eps)
         assert abs(grad[r, c] - fd) <= 1e-5 * max(abs(fd), 1e-8), ((r, c), grad[r, c], fd)
+
+
+def test_torch_backward_through_the_function():
+    """loss.backward() through RoeExnerSteps runs the adjoint kernels: the gradient equals
+    the direct reverse-mode call (to 1e-12: the adjoint's atomic sums make the last bits
+    depend on the order in which the GPU adds them)."""
+    from pyexner_b200.tangent import RoeExnerSteps, StepsSpec, vjp_run
+
+    bundle, cfg, mask, st = setup(*smooth_case())
+    spec = StepsSpec(mask, cfg, st.seds, 4, "SSPRK2", 0.5)
+    planes = [getattr(st, f).clone().requires_grad_(f in ("h", "hu", "hv", "z_b", "G")) for f in st.PLANES]
+    out = RoeExnerSteps.apply(spec, *planes)
+    zb_out = out[st.PLANES.index("z_b")]
+    loss = (zb_out ** 2).sum() + out[0].sum()
+    loss.backward()
+    abar = st.clone()
+    for f in st.PLANES:
+        getattr(abar, f).zero_()
+    abar.z_b.copy_(2 * zb_out.detach())
+    abar.h.fill_(1.0)
+    vjp_run(st, abar, mask, cfg, 4, "SSPRK2", 0.5)
+    ref = abar.to_numpy()
+    for k, f in enumerate(st.PLANES):
+        if f in ("h", "hu", "hv", "z_b", "G"):
+            assert rel_err(planes[k].grad.cpu().numpy(), ref[f]) <= 1e-12, f
