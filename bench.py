@@ -19,6 +19,8 @@ Reported:
   accuracy   rel-L1 of h and z+z_b, float32 vs float64 after the accuracy run;
   cpu_baseline  the float64 C/OpenMP oracle (all host threads) on a 512 x 512 sample of
              the same generator, about 10 s of CPU work;
+  plain_roe  configuration 1: the plain Roe dam-break (256^2, float64, SSPRK2, 200 steps)
+             and the NumPy oracle on the host for 10 steps of it;
   ensemble   the ragged ensemble workload (64 Roe-Exner dam breaks, sides U{128..1024},
              own beds, step heights and dts; float32; 1000 SSPRK2 steps): autotuned band
              height, cell-updates/s over all members (state ~1.1 GB, larger than L2).
@@ -352,6 +354,46 @@ def ensemble_run(count, steps, seed=0):
             "dt_range": [float(d.min()), float(d.max())], "l2": "state ~1.1 GB, larger than L2"}
 
 
+def plain_roe_run(steps=200, cpu_steps=10):
+    """Configuration 1: the plain Roe dam-break, 256 x 256 cells, float64, SSPRK2, 200
+    steps through ``run_steps`` (graph replay), and the float64 NumPy oracle on the host
+    for ``cpu_steps`` steps of the same case (single thread)."""
+    import torch
+
+    from oracle import boundaries as OB
+    from oracle import integrators as OI
+    from pyexner_b200 import BoundaryManager, RoeState, cases, create_solver_bundle, run_steps
+
+    c = cases.dambreak_roe(256)
+    params = dict(flux_scheme="Roe", boundaries=c["params"]["boundaries"])
+    bm = BoundaryManager(params, c["X"], c["Y"])
+    st = RoeState.from_numpy(c["arrs"], torch.float64)
+    bundle = create_solver_bundle("Roe")
+    cfg = bundle.config(st, None, bm, c["dx"], params)
+    mask = bundle.mask_fn(st)
+    st = bundle.init_fn(st, mask, cfg)
+    warm = st.clone()
+    run_steps(warm, mask, cfg, "SSPRK2", steps, 0.5, log_dt=False)  # captures the step graph
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    run_steps(st, mask, cfg, "SSPRK2", steps, 0.5, log_dt=False)
+    e1.record()
+    e1.synchronize()
+    sec = e0.elapsed_time(e1) / 1e3
+    cells = 256 * 256
+    obcs = OB.Boundaries("Roe", c["params"]["boundaries"], c["X"], c["Y"])
+    arrs = {k: np.array(v) for k, v in c["arrs"].items()}
+    t = time.perf_counter()
+    OI.run_roe(arrs, obcs, c["dx"], 0.5, cpu_steps, "SSPRK2")
+    cpu = cells * cpu_steps / (time.perf_counter() - t)
+    return {"workload": "roe_dambreak_256x256_reflective_ssprk2_f64", "steps": steps, "value": cells * steps / sec,
+            "unit": UNIT, "ms_per_step": 1e3 * sec / steps,
+            "cpu_oracle": {"value": cpu, "unit": UNIT, "cores": 1, "kind": "port",
+                           "sample": f"{cpu_steps} SSPRK2 steps of the same case, float64 NumPy oracle"}}
+
+
 def _oracle_case(n):
     from oracle import boundaries as OB
     from oracle import c_oracle as CO
@@ -519,6 +561,7 @@ def main():
     e2e_val = ncell * args.steps / e2e_sec
     acc = accuracy_run(n, args.accuracy_steps) if args.accuracy_steps > 0 else None
     ens = ensemble_run(args.ensemble_members, args.ensemble_steps) if args.ensemble_members > 0 else None
+    roe = plain_roe_run() if rank == 0 and not args.no_cpu else None
     if rank != 0:
         if world > 1:
             dist.barrier()
@@ -542,6 +585,7 @@ def main():
         "fp64": {"value": value64, "unit": UNIT, "fp32_over_fp64": value / world / value64},
         "bandwidth_case": big,
         "ensemble": ens,
+        "plain_roe": roe,
         "accuracy": acc,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
