@@ -307,13 +307,17 @@ Geometry stage_geometry(int ny, int nx, int resident_warps, int want_rows) {
         // enough bands to give every resident warp an item, but no band taller than 128
         // rows: on large grids several waves of shorter bands keep the concurrently active
         // items close together in memory (halo rows and columns shared through L2)
-        const int target_bands = std::max(1, resident_warps / g.nstrips);
+        const int target_bands = std::max(1, resident_warps / pxb_stage_items_per_band(g.nstrips));
         rows = std::max(8, std::min(128, (ny - 1 + target_bands - 1) / target_bands));
     }
     g.band_rows = rows;
     g.nbands = std::max(1, (ny - 1 + rows - 1) / rows);
-    const int items = g.nstrips * g.nbands;
-    g.grid = std::max(1, (items + 3) / 4);
+    const int items = pxb_stage_items_per_band(g.nstrips) * g.nbands;
+    // Unless the grid is small, launch exactly the resident capacity: every SM then holds
+    // the same number of blocks (a grid a little below capacity is spread unevenly by the
+    // block scheduler), and the kernel's work queue hands out the items beyond one per warp.
+    const int need = std::max(1, (items + 3) / 4), cap = std::max(1, resident_warps / 4);
+    g.grid = need >= cap / 4 ? cap : need;
     return g;
 }
 
@@ -764,6 +768,7 @@ int re_stage_impl(pxb_re_plan* P, const pxb_re_fields* in, const pxb_re_fields* 
     a.nstrips = g.nstrips;
     a.nbands = g.nbands;
     a.err = &P->c.scr->err;
+    a.queue = P->c.scr->queue;
     PXB_CUDA(pxb::launch_re_stage<T>(a, P->mpm != 0, P->nodata != nullptr, avg != nullptr, g.grid, s));
     return PXB_OK;
 }
@@ -1148,7 +1153,7 @@ int ens_build_stage_tables(pxb_re_ens* E) {
         t[2].push_back(ens_stage_args<T>(E, k, &mb.b, &mb.a, &mb.a, &mb.a));
         t[3].push_back(ens_stage_args<T>(E, k, &mb.a, &b_noG, nullptr, &mb.a));
         const pxb::REStageArgs<T>& a = t[0].back();
-        base.push_back(base.back() + a.nstrips * a.nbands);
+        base.push_back(base.back() + pxb_stage_items_per_band(a.nstrips) * a.nbands);
     }
     for (int v = 0; v < 4; ++v) {
         if (!E->st_args[v]) PXB_CUDA(cudaMalloc(&E->st_args[v], sizeof(pxb::REStageArgs<T>) * E->nm));
@@ -1211,6 +1216,7 @@ int ens_stage_launch(pxb_re_ens* E, int v, cudaStream_t s) {
     a.args = (const pxb::REStageArgs<T>*)E->st_args[v];
     a.base = E->st_base;
     a.nmembers = E->nm;
+    a.queue = E->scr[0].queue;
     const bool avg = v == 2;
     const int grid = std::max(1, std::min((E->st_total + 3) / 4, std::max(1, E->bps[avg ? 1 : 0]) * E->sm_count));
     PXB_CUDA(pxb::launch_ens_stage<T>(a, E->mpm != 0, E->has_mask, avg, grid, s));

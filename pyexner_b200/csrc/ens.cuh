@@ -2,11 +2,12 @@
 // boundary recipes and dt) advanced together, one launch per phase for all members.
 //
 // The work items of every member (32-column strips x row bands, as in the single-grid
-// kernels) are numbered consecutively, member after member; a persistent grid strides
-// over the global item range.  A warp finds the member of its item by binary search in
-// the item offsets and keeps that member's argument block in a shared-memory slot of its
-// own, refreshed only when the member changes, so the per-item body is exactly the
-// single-grid one (re_stage_item / re_cfl_item) reading its arguments from shared memory.
+// kernels) are numbered consecutively, member after member; a persistent grid covers the
+// global item range (first item by warp index, the rest from a work queue).  A warp finds
+// the member of its item by binary search in the item offsets and keeps that member's
+// argument block in a shared-memory slot of its own, refreshed only when the member
+// changes, so the per-item body is exactly the single-grid one (re_stage_item /
+// re_cfl_item) reading its arguments from shared memory.
 //
 // CFL: each item folds its face speeds into the member's maximum (one 64-bit atomicMax
 // per warp and item); a one-thread-per-member launch then turns the maxima into the
@@ -23,6 +24,7 @@ struct EnsStageArgs {
     const REStageArgs<T>* args;  // per member
     const int* base;             // item offset of each member, nmembers + 1 entries
     int nmembers;
+    unsigned int* queue;         // {next dynamic item, finished blocks}, zero between launches
 };
 
 template <class T>
@@ -54,16 +56,18 @@ __device__ __forceinline__ void ens_load_slot(A* slot, const A* src) {
     __syncwarp();
 }
 
+// Items beyond one per warp come from a grid-wide queue, as in re_stage_kernel.
 template <class T, bool MPM, bool HAS_MASK, bool AVG>
 __global__ void __launch_bounds__(128, PXB_STAGE_BOUNDS(T, AVG)) ens_stage_kernel(const EnsStageArgs<T> e) {
     __shared__ REStageArgs<T> slot[4];
     const int w = threadIdx.x >> 5;
-    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     const int total = __ldg(e.base + e.nmembers);
     int cur = -1;
     bool bad = false;
-    for (int item = wid; item < total; item += nw) {
+    int item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    while (item < total) {
         const int m = ens_member_of(e.base, e.nmembers, item);
         if (m != cur) {
             if (bad) atomicOr(slot[w].err, 1);
@@ -72,8 +76,19 @@ __global__ void __launch_bounds__(128, PXB_STAGE_BOUNDS(T, AVG)) ens_stage_kerne
             cur = m;
         }
         re_stage_item<T, MPM, HAS_MASK, AVG>(slot[w], item - __ldg(e.base + m), bad);
+        unsigned next = 0;
+        if (lane == 0) next = atomicAdd(&e.queue[0], 1u);
+        item = nw + (int)__shfl_sync(FULL, next, 0);
     }
     if (bad) atomicOr(slot[w].err, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&e.queue[1], 1u) == gridDim.x - 1) {
+            atomicExch(&e.queue[0], 0u);
+            atomicExch(&e.queue[1], 0u);
+        }
+    }
 }
 
 template <class T, bool HAS_MASK>

@@ -59,6 +59,20 @@ __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(
 template <class T>
 __host__ __device__ constexpr bool is_f32() { return sizeof(T) == 4; }
 
+// Sums of several products.  The float build contracts a * b + c into one FMA, but a
+// sum of two products can be contracted either way and the compiler's choice depends on
+// the code around the inlined expression, so two kernels sharing a formula could differ
+// in the last bit.  Such sums are spelled out here:
+//   sum2 / dif2: both products rounded on their own, then added (mirror states at
+//                reflective walls cancel exactly, as in the reference's arithmetic);
+//   fsum2:       a * b fused onto the rounded c * d (sums of squares, no cancellation).
+// In the float64 build (--fmad=false) all three are the plain expression.
+template <class T>
+__device__ __forceinline__ T sum2(T a, T b, T c, T d) { return mul_rn(a, b) + mul_rn(c, d); }
+template <class T>
+__device__ __forceinline__ T dif2(T a, T b, T c, T d) { return mul_rn(a, b) - mul_rn(c, d); }
+__device__ __forceinline__ float fsum2(float a, float b, float c, float d) { return __fmaf_rn(a, b, __fmul_rn(c, d)); }
+
 // ---------------------------------------------------------------- hydrodynamic faces
 // Per-cell values used by the Roe-Exner face flux (roe_exner.py:317-335, 421-425, 455).
 template <class T>
@@ -79,12 +93,13 @@ __device__ __forceinline__ HCell<T> make_hcell(T h, T hu, T hv, T zb, T z, T nb)
     const bool wet = hc > T(DRY_TOL);
     p.h = hc;
     if constexpr (is_f32<T>()) {
+        // per-cell values are rounded products (mul_rn): no later sum can fuse them
         const float rs = f_rsqrt(hc);
         const float r = rs * rs;
-        p.u = wet ? hu * r : 0.f;
-        p.v = wet ? hv * r : 0.f;
-        p.sq = hc * rs;
-        p.c = 3.1320919526731650f * p.sq;  // sqrt(g) sqrt(h)
+        p.u = wet ? mul_rn(hu, r) : 0.f;
+        p.v = wet ? mul_rn(hv, r) : 0.f;
+        p.sq = mul_rn(hc, rs);
+        p.c = mul_rn(3.1320919526731650f, p.sq);  // sqrt(g) sqrt(h)
     } else {
         p.u = wet ? hu / hc : T(0);
         p.v = wet ? hv / hc : T(0);
@@ -111,9 +126,9 @@ __device__ __forceinline__ void roe_exner_face(const HCell<T>& I, const HCell<T>
         const float rden = f_rcp(den);
         const float gh = 9.81f * ht;
         rct = f_rsqrt(gh);
-        ct = gh * rct;
-        ut = (uhi * I.sq + uhj * J.sq) * rden;
-        vt = (vhi * I.sq + vhj * J.sq) * rden;
+        ct = mul_rn(gh, rct);
+        ut = sum2(uhi, I.sq, uhj, J.sq) * rden;
+        vt = sum2(vhi, I.sq, vhj, J.sq) * rden;
     } else {
         ct = d_sqrt(T(G_ACC) * ht);
         ut = (uhi * I.sq + uhj * J.sq) / den;
@@ -145,10 +160,10 @@ __device__ __forceinline__ void roe_exner_face(const HCell<T>& I, const HCell<T>
         }
     }
     const T dh = J.h - I.h;
-    const T dhu = J.h * uhj - I.h * uhi;
-    const T dhv = J.h * vhj - I.h * vhi;
+    const T dhu = dif2(J.h, uhj, I.h, uhi);
+    const T dhv = dif2(J.h, vhj, I.h, vhi);
     const T dz = J.zt - I.zt;
-    const T thrust = -T(G_ACC) * ht * dz;
+    const T thrust = mul_rn(-T(G_ACC) * ht, dz);
     const T nt = T(0.5) * (I.nb + J.nb);
     T a1, a2, a3, b1;
     if constexpr (is_f32<T>()) {
@@ -158,9 +173,9 @@ __device__ __forceinline__ void roe_exner_face(const HCell<T>& I, const HCell<T>
         a3 = (l1r * dh - dhu) * r2;
         // h^(-4/3) with the DRY_TOL floor of h^(4/3) (h^(4/3) < DRY_TOL  <=>  h < DRY_TOL^(3/4))
         const float rp = ht < 1e-3f ? 1e4f : f_ex2(-1.3333333333f * f_lg2(ht));
-        const float sf = nt * nt * f_sqrt(ut * ut + vt * vt) * ut * rp;
-        const float tau = 9.81f * ht * sf * dx;
-        b1 = (thrust - tau) * r2;
+        const float sf = nt * nt * f_sqrt(fsum2(ut, ut, vt, vt)) * ut * rp;
+        const float tau = mul_rn(9.81f * ht * sf, dx);
+        b1 = mul_rn(thrust - tau, r2);
     } else {
         const T den2 = T(-2.0) * ct;
         a1 = (-l3r * dh + dhu) / den2;
@@ -178,18 +193,19 @@ __device__ __forceinline__ void roe_exner_face(const HCell<T>& I, const HCell<T>
         // T_k = w_k + e_k (k = 1, 3; e_k = lambda_E,k alpha_k, zero without the fix):
         //   upwP = (A1 + A3, A1 l1 + A3 l3, (A1 + A3) vt + [ut > 0] w2 ct)
         //   upwM = the same with T_k - A_k and [ut <= 0].
-        const float w1 = l1 * a1 - b1, w2c = ut * a2 * ct, w3 = l3 * a3 - b3;
-        const float e1 = lE1 * a1, e3 = lE3 * a3;
+        // (b1, w2c, e1, e3 are rounded products, so each sum below has one product to fuse)
+        const float w1 = __fmaf_rn(l1, a1, -b1), w2c = mul_rn(ut * a2, ct), w3 = __fmaf_rn(l3, a3, -b3);
+        const float e1 = mul_rn(lE1, a1), e3 = mul_rn(lE3, a3);
         const float A1 = (l1 > 0.f ? w1 : 0.f) + (lE1 > 0.f ? e1 : 0.f);
         const float A3 = (l3 > 0.f ? w3 : 0.f) + (lE3 > 0.f ? e3 : 0.f);
         const float B1 = (w1 + e1) - A1, B3 = (w3 + e3) - A3;
         const bool s2 = ut > 0.f;
         p0 = A1 + A3;
-        p1 = A1 * l1 + A3 * l3;
-        p2 = p0 * vt + (s2 ? w2c : 0.f);
+        p1 = sum2(A1, l1, A3, l3);
+        p2 = __fmaf_rn(p0, vt, s2 ? w2c : 0.f);
         n0 = B1 + B3;
-        n1 = B1 * l1 + B3 * l3;
-        n2 = n0 * vt + (s2 ? 0.f : w2c);
+        n1 = sum2(B1, l1, B3, l3);
+        n2 = __fmaf_rn(n0, vt, s2 ? 0.f : w2c);
     } else {
     {
         const T w = l1 * a1 - b1;
@@ -251,15 +267,16 @@ __device__ __forceinline__ ECell<T> make_ecell(T h, T hu, T hv, T zb, T G) {
     if constexpr (is_f32<T>()) {
         const float rs = f_rsqrt(he);
         const float r = rs * rs;
-        e.sq = he * rs;
-        e.u = wet ? hu * r : 0.f;
-        e.v = wet ? hv * r : 0.f;
+        e.sq = mul_rn(he, rs);
+        e.u = wet ? mul_rn(hu, r) : 0.f;
+        e.v = wet ? mul_rn(hv, r) : 0.f;
     } else {
         e.sq = d_sqrt(he);
         e.u = wet ? hu / he : T(0);
         e.v = wet ? hv / he : T(0);
     }
-    e.um = e.u * e.u + e.v * e.v;
+    if constexpr (is_f32<T>()) e.um = fsum2(e.u, e.u, e.v, e.v);
+    else e.um = e.u * e.u + e.v * e.v;
     e.G = G;
     return e;
 }
@@ -268,8 +285,8 @@ template <class T, bool YF>
 __device__ __forceinline__ T exner_face(const ECell<T>& I, const ECell<T>& J) {
     const T uhi = YF ? -I.v : I.u;
     const T uhj = YF ? -J.v : J.u;
-    const T qi = I.G * I.um * uhi;
-    const T qj = J.G * J.um * uhj;
+    const T qi = mul_rn(I.G * I.um, uhi);
+    const T qj = mul_rn(J.G * J.um, uhj);
     const T gt = T(0.5) * (I.G + J.G);
     const T dz = J.zbe - I.zbe;
     const T qbi = qi + (gt - I.G) * I.um * uhi;
@@ -335,7 +352,7 @@ __device__ __forceinline__ T mpm_grass(T h, T hu, T hv, bool nodata, const SedTa
         rs = rs * (1.5f - 0.5f * hc * rs * rs);
         const float r = rs * rs;
         const float u = hu * r, v = hv * r;
-        const float vel2 = u * u + v * v;
+        const float vel2 = fsum2(u, u, v, v);
         float rcb = f_ex2(-0.33333333333f * f_lg2(hc));  // h^(-1/3)
         rcb = rcb * (4.f - hc * rcb * rcb * rcb) * (1.f / 3.f);
         float G = 0.f;
@@ -399,9 +416,9 @@ __device__ __forceinline__ CCell<T> make_ccell(T h, T hu, T hv, T G) {
     if constexpr (is_f32<T>()) {
         p.rs = f_rsqrt(p.h);
         const float r = p.rs * p.rs;
-        p.sq = p.h * p.rs;
-        p.u = hu * r;
-        p.v = hv * r;
+        p.sq = mul_rn(p.h, p.rs);
+        p.u = mul_rn(hu, r);
+        p.v = mul_rn(hv, r);
     } else {
         p.rs = T(0);
         p.sq = d_sqrt(p.h);
@@ -426,10 +443,10 @@ __device__ __forceinline__ void cubic_extremes(T ut, T at, T ct, T& lmin, T& lma
         // together) the trigonometric form loses digits, so those faces redo the
         // solve in float64.
         const float b = -2.f * ut;
-        const float c = (1.f + at) * (ct * ct) - ut * ut;
+        const float c = dif2(1.f + at, ct * ct, ut, ut);
         const float d = -(ct * ct) * at * ut;
-        const float p = (-3.f * c - b * b) * (1.f / 3.f);
-        const float q = (2.f * b * b * b + 9.f * b * c + 27.f * d) * (-1.f / 27.f);
+        const float p = dif2(-3.f, c, b, b) * (1.f / 3.f);
+        const float q = (mul_rn(2.f * b * b, b) + mul_rn(9.f * b, c) + mul_rn(27.f, d)) * (-1.f / 27.f);
         // (3q / 2p) sqrt(-3/p); p < 0 for three real roots, otherwise this is NaN and the
         // float64 solve below takes over
         const float rp = f_rcp(p);
@@ -443,13 +460,13 @@ __device__ __forceinline__ void cubic_extremes(T ut, T at, T ct, T& lmin, T& lma
         }
         const float th = acosf(xr);
         const float sq = 2.f * f_sqrt(-p * (1.f / 3.f));
-        const float shift = b * (1.f / 3.f);
+        const float shift = mul_rn(b, 1.f / 3.f);
         // th / 3 is in [0, pi/3]: the hardware sine / cosine are within 2^-21 absolute there
         float sn, cs;
         __sincosf(th * (1.f / 3.f), &sn, &cs);
-        lmax = sq * cs + shift;
+        lmax = __fmaf_rn(sq, cs, shift);
         // cos((th + 2 pi)/3) = -cos(th/3)/2 - sqrt(3)/2 sin(th/3)
-        lmin = sq * (-0.5f * cs - 0.86602540378f * sn) + shift;
+        lmin = __fmaf_rn(sq, __fmaf_rn(-0.5f, cs, -mul_rn(0.86602540378f, sn)), shift);
         return;
     }
     const T b = T(-2) * ut;
@@ -476,9 +493,10 @@ __device__ __forceinline__ T face_speed(const CCell<T>& I, const CCell<T>& J) {
     const T gt = T(0.5) * (I.G + J.G);
     T ut, ct, at;
     if constexpr (is_f32<T>()) {
-        ut = (uhi * I.sq + uhj * J.sq) * f_rcp(den);
+        ut = sum2(uhi, I.sq, uhj, J.sq) * f_rcp(den);
         ct = f_sqrt(9.81f * ht);
-        at = gt * (uhi * uhi + uhi * uhj + uhj * uhj + vhi * vhj) * (I.rs * J.rs);
+        const float s4 = __fmaf_rn(vhi, vhj, __fmaf_rn(uhj, uhj, fsum2(uhi, uhi, uhi, uhj)));
+        at = gt * s4 * (I.rs * J.rs);
     } else {
         ut = (uhi * I.sq + uhj * J.sq) / den;
         ct = d_sqrt(T(G_ACC) * ht);

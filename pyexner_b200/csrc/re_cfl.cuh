@@ -24,6 +24,7 @@ struct CflScratch {
     int pad;
     double t_step;               // simulation time at the start of the current step
     double t_next;               // t_step + dt: the time the next dt is added to
+    unsigned int queue[2];       // stage kernel work queue: items handed out, blocks finished
 };
 
 // Start of a fixed-step run at time t0 (the first CFL launch moves it into t_step).

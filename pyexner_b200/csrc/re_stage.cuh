@@ -57,6 +57,7 @@ struct REStageArgs {
     SedTable<T> sed;
     int band_rows, nstrips, nbands;
     int* err;
+    unsigned int* queue;  // {next dynamic item, finished blocks}, zero between launches
 };
 
 // Asynchronous global -> shared copies of one element (cp.async, completion by group).
@@ -66,7 +67,19 @@ __device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
     if constexpr (sizeof(T) == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
     else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+static_assert(sizeof(pxb_ring_recipe) == 48, "ring recipes are copied as three 16-byte chunks");
+
+// Fields of the second boundary application (z_b and G donors) packed into one word by
+// the first: flags bits 3-4 and the four offsets (each in [-1, 1]) biased by 8.
+__device__ __forceinline__ unsigned pack_zg(unsigned flags, int zdy, int zdx, int gdy, int gdx) {
+    return (flags & 24u) | ((unsigned)(zdy + 8) << 8) | ((unsigned)(zdx + 8) << 12) | ((unsigned)(gdy + 8) << 16) |
+           ((unsigned)(gdx + 8) << 20);
+}
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
@@ -114,16 +127,24 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
     const T dtdx = dt / dx;  // float path only
     const T DRY = T(DRY_TOL);
     {
-        const int band = item / a.nstrips;
-        const int strip = item - band * a.nstrips;
+        const int ipb = pxb_stage_items_per_band(a.nstrips);
+        const int band = item / ipb;
+        const int k = item - band * ipb;
+        int strip = k - 1, half = -1;  // half: 0 / 1 = upper / lower half of a boundary strip
+        if (ipb == 1) strip = 0;
+        else if (k < 2) { strip = 0; half = k; }
+        else if (k >= a.nstrips) { strip = a.nstrips - 1; half = k - a.nstrips; }
         const int c = strip * PXB_STRIP_OUT - PXB_HALO + lane;
         const bool colok = (c >= 0) && (c < nx);
         const bool has_e = colok && (c + 1 < nx) && (lane < 31);
         const bool last_strip = strip == a.nstrips - 1;
         const bool out_col = colok && lane >= PXB_HALO && (lane < PXB_HALO + PXB_STRIP_OUT || last_strip);
         const bool interior_col = (c >= 1) && (c <= nx - 2);
-        const int R0 = band * a.band_rows;
-        const int R1 = (band == a.nbands - 1) ? ny : R0 + a.band_rows;
+        const int B0 = band * a.band_rows;
+        const int B1 = (band == a.nbands - 1) ? ny : B0 + a.band_rows;
+        const int Bm = B0 + (B1 - B0 + 1) / 2;
+        const int R0 = half == 1 ? Bm : B0;
+        const int R1 = half == 0 ? Bm : B1;
         const int L0 = max(0, R0 - 3), L1 = min(ny, R1 + 3);
         // boundary recipes can only apply in the first/last strip or on rows 0 / ny-1
         const bool bc_strip = (a.ring != nullptr) && (strip == 0 || last_strip);
@@ -215,6 +236,33 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
         };
         if (ASYNC_PARTNER) partner_copy(L0);
         cp_async_commit();
+        // Boundary recipes (first / last strip, first / last row): the recipe of the row
+        // that the first boundary application treats in iteration r (q = r-3) is copied
+        // into this warp's shared buffer during iteration r-1, so no recipe load is waited
+        // on inside the pipeline; the first application leaves the z_b / G fields of the
+        // second (row p = r-5, two iterations later) in a packed word.  Float32 only, as
+        // the row copies.
+        constexpr bool ASYNC_RECIPES = ASYNC_ROWS;
+        __shared__ __align__(16) pxb_ring_recipe rcbuf[4][ASYNC_RECIPES ? 2 : 1][32];
+        __shared__ unsigned zgbuf[4][ASYNC_RECIPES ? 4 : 1][32];
+        pxb_ring_recipe(*rcb)[32] = rcbuf[threadIdx.x >> 5];
+        unsigned(*zgb)[32] = zgbuf[threadIdx.x >> 5];
+        auto recipe_copy = [&](const int rr) {  // the recipes used in iteration rr
+            const int qn = rr - 3;
+            if (qn >= L0 && qn < L1 && (bc_strip || (bc_rows && (qn == 0 || qn == ny - 1)))) {
+                const int slot = colok ? ring_slot(qn, c, ny, nx) : -1;
+                pxb_ring_recipe* d = &rcb[rr & 1][lane];
+                if (slot >= 0) {
+                    const char* src = reinterpret_cast<const char*>(a.ring + slot);
+                    char* dst = reinterpret_cast<char*>(d);
+                    cp_async16(dst, src);
+                    cp_async16(dst + 16, src + 16);
+                    cp_async16(dst + 32, src + 32);
+                } else {
+                    d->flags = 0u;
+                }
+            }
+        };
 
         // One pipeline iteration.  In the steady state (rows L0+5 .. L1-1) every phase has
         // valid rows, so the row checks compile away.
@@ -239,6 +287,7 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
             const bool m_r = nm;
             load_row(r + 1);
             if (ASYNC_PARTNER) partner_copy(r + 1);
+            if (ASYNC_RECIPES) recipe_copy(r + 1);
             cp_async_commit();
             T pah = 0, pahu = 0, pahv = 0, pazb = 0, paG = 0;
             if (ASYNC_PARTNER) {
@@ -340,22 +389,32 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
             T hbh = hf3h, hbu = hf3u, hbv = hf3v, zb1 = zin3, gb1 = gin3;
             T sbh = hf3h, sbu = hf3u, sbv = hf3v;
             if (rowD && (bc_strip || (bc_rows && (q == 0 || q == ny - 1)))) {
-                const int slot = colok ? ring_slot(q, c, ny, nx) : -1;
                 unsigned flags = 0;
                 int hdy = 0, hdx = 0, mdy = 0, mdx = 0, zdy = 0, zdx = 0, gdy = 0, gdx = 0;
                 T m0 = 0, m1 = 0, m2c = 0, m3 = 0;
-                if (slot >= 0) {
-                    const pxb_ring_recipe& rc = a.ring[slot];
+                auto take = [&](const pxb_ring_recipe& rc) {
                     flags = rc.flags;
                     hdy = rc.h_dy; hdx = rc.h_dx; mdy = rc.m_dy; mdx = rc.m_dx;
                     zdy = rc.zb_dy; zdx = rc.zb_dx; gdy = rc.g_dy; gdx = rc.g_dx;
                     m0 = T(rc.m[0]); m1 = T(rc.m[1]); m2c = T(rc.m[2]); m3 = T(rc.m[3]);
+                };
+                if constexpr (ASYNC_RECIPES) {
+                    const pxb_ring_recipe& rc = rcb[r & 1][lane];  // copied in iteration r-1
+                    if (rc.flags != 0u) take(rc);
+                    zgb[r & 3][lane] = pack_zg(flags, zdy, zdx, gdy, gdx);
+                } else {
+                    const int slot = colok ? ring_slot(q, c, ny, nx) : -1;
+                    if (slot >= 0) take(a.ring[slot]);
                 }
                 if (__any_sync(FULL, flags != 0)) {
-                    // donor value at (row q+dy, column c+dx); the row is chosen by the receiver
+                    // Donor value at (row q+dy, column c+dx); the row is chosen by the
+                    // receiver.  Donors lie in another row only for cells of the first and
+                    // last rows (plan creation checks it), so other rows shuffle one value.
+                    const bool dyrow = (q == 0) || (q == ny - 1);
                     auto fetch = [&](int dy, int dx_, T above, T mid, T below) {
-                        const T va = __shfl_sync(FULL, above, lane + dx_);
                         const T vm = __shfl_sync(FULL, mid, lane + dx_);
+                        if (!dyrow) return vm;
+                        const T va = __shfl_sync(FULL, above, lane + dx_);
                         const T vb = __shfl_sync(FULL, below, lane + dx_);
                         return pick_row(dy, va, vm, vb);
                     };
@@ -366,7 +425,7 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
                     if (flags & 1u) hbh = vh;
                     if (flags & 2u) {
                         if (flags & 4u) { hbu = m0; hbv = m1; }
-                        else { hbu = m0 * vu + m1 * vv; hbv = m2c * vu + m3 * vv; }
+                        else { hbu = sum2(m0, vu, m1, vv); hbv = sum2(m2c, vu, m3, vv); }
                     }
                     if (flags & 8u) zb1 = vz;
                     if (!MPM) {
@@ -382,8 +441,8 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
                     sbv = hbv;
                     if (flags & 1u) sbh = wh;
                     if ((flags & 2u) && !(flags & 4u)) {
-                        sbu = m0 * wu + m1 * wv;
-                        sbv = m2c * wu + m3 * wv;
+                        sbu = sum2(m0, wu, m1, wv);
+                        sbv = sum2(m2c, wu, m3, wv);
                     }
                 }
             }
@@ -429,21 +488,33 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
             const bool rowG = S || ((p >= L0) && (p < L1));
             T zfin = zbp5, gfin = gg5;
             if (rowG && (bc_strip || (bc_rows && (p == 0 || p == ny - 1)))) {
-                const int slot = colok ? ring_slot(p, c, ny, nx) : -1;
                 unsigned flags = 0;
                 int zdy = 0, zdx = 0, gdy = 0, gdx = 0;
-                if (slot >= 0) {
-                    const pxb_ring_recipe& rc = a.ring[slot];
-                    flags = rc.flags;
-                    zdy = rc.zb_dy; zdx = rc.zb_dx; gdy = rc.g_dy; gdx = rc.g_dx;
+                if constexpr (ASYNC_RECIPES) {
+                    const unsigned w = zgb[(r - 2) & 3][lane];  // left by the first application of row p
+                    flags = w & 24u;
+                    zdy = (int)((w >> 8) & 15u) - 8;
+                    zdx = (int)((w >> 12) & 15u) - 8;
+                    gdy = (int)((w >> 16) & 15u) - 8;
+                    gdx = (int)((w >> 20) & 15u) - 8;
+                } else {
+                    const int slot = colok ? ring_slot(p, c, ny, nx) : -1;
+                    if (slot >= 0) {
+                        const pxb_ring_recipe& rc = a.ring[slot];
+                        flags = rc.flags;
+                        zdy = rc.zb_dy; zdx = rc.zb_dx; gdy = rc.g_dy; gdx = rc.g_dx;
+                    }
                 }
                 if (__any_sync(FULL, (flags & 24u) != 0)) {
-                    const T z6 = __shfl_sync(FULL, zbp6, lane + zdx), z5 = __shfl_sync(FULL, zbp5, lane + zdx);
-                    const T z4 = __shfl_sync(FULL, zbp4, lane + zdx);
-                    const T g6 = __shfl_sync(FULL, gg6, lane + gdx), g5 = __shfl_sync(FULL, gg5, lane + gdx);
-                    const T g4 = __shfl_sync(FULL, gg4, lane + gdx);
-                    if (flags & 8u) zfin = pick_row(zdy, z6, z5, z4);
-                    if (flags & 16u) gfin = pick_row(gdy, g6, g5, g4);
+                    T zv = __shfl_sync(FULL, zbp5, lane + zdx), gv = __shfl_sync(FULL, gg5, lane + gdx);
+                    if ((p == 0) || (p == ny - 1)) {  // donors in another row: first / last row only
+                        const T z6 = __shfl_sync(FULL, zbp6, lane + zdx), z4 = __shfl_sync(FULL, zbp4, lane + zdx);
+                        const T g6 = __shfl_sync(FULL, gg6, lane + gdx), g4 = __shfl_sync(FULL, gg4, lane + gdx);
+                        zv = pick_row(zdy, z6, zv, z4);
+                        gv = pick_row(gdy, g6, gv, g4);
+                    }
+                    if (flags & 8u) zfin = zv;
+                    if (flags & 16u) gfin = gv;
                 }
             }
             if (rowG && p >= R0 && p < R1 && out_col) {
@@ -503,14 +574,32 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
     }
 }
 
+// The grid is sized to the resident capacity of the device.  A warp's first item is its
+// warp index; further items come from a grid-wide queue (one atomic per item), so warps
+// on lightly loaded SMs take more of them and no SM waits on a fixed share.  The last
+// block to finish resets the queue for the next launch on the stream.
 template <class T, bool MPM, bool HAS_MASK, bool AVG>
 __global__ void __launch_bounds__(128, PXB_STAGE_BOUNDS(T, AVG)) re_stage_kernel(const REStageArgs<T> a) {
-    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
-    const int nitems = a.nstrips * a.nbands;
+    const int nitems = pxb_stage_items_per_band(a.nstrips) * a.nbands;
     bool bad = false;
-    for (int item = wid; item < nitems; item += nw) re_stage_item<T, MPM, HAS_MASK, AVG>(a, item, bad);
+    int item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    while (item < nitems) {
+        re_stage_item<T, MPM, HAS_MASK, AVG>(a, item, bad);
+        unsigned next = 0;
+        if (lane == 0) next = atomicAdd(&a.queue[0], 1u);
+        item = nw + (int)__shfl_sync(FULL, next, 0);
+    }
     if (bad) atomicOr(a.err, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&a.queue[1], 1u) == gridDim.x - 1) {
+            atomicExch(&a.queue[0], 0u);
+            atomicExch(&a.queue[1], 0u);
+        }
+    }
 }
 
 }  // namespace pxb
