@@ -26,18 +26,26 @@
 #include "pxb_device.cuh"
 
 // Resident 128-thread blocks per SM the build is register-limited to (tuning knobs,
-// measured on the 2048^2 and 8192^2 Gaussian-bed cases): 5 (96 registers) for both the
-// plain stage and the averaging second SSPRK2 stage.
+// measured on the 2048^2 and 8192^2 Gaussian-bed cases): 4 (128 registers, no spills)
+// for both the plain stage and the averaging second SSPRK2 stage; 5 (96 registers) is
+// 1% faster at 8192^2 and 4% slower at 2048^2, where fewer resident warps mean taller
+// bands and fewer redundant halo rows.
 #ifndef PXB_STAGE_MIN_BLOCKS
-#define PXB_STAGE_MIN_BLOCKS 5
+#define PXB_STAGE_MIN_BLOCKS 4
 #endif
 #ifndef PXB_STAGE_MIN_BLOCKS_AVG
-#define PXB_STAGE_MIN_BLOCKS_AVG 5
+#define PXB_STAGE_MIN_BLOCKS_AVG 4
 #endif
 // float64 state (twice the registers per value)
 #ifndef PXB_STAGE_MIN_BLOCKS_F64
 #define PXB_STAGE_MIN_BLOCKS_F64 5
 #endif
+// Unroll factor of the steady row loop (tuning knob).
+#ifndef PXB_STAGE_UNROLL
+#define PXB_STAGE_UNROLL 1
+#endif
+#define PXB_PRAGMA(x) _Pragma(#x)
+#define PXB_UNROLL(n) PXB_PRAGMA(unroll n)
 #define PXB_STAGE_BOUNDS(T, AVG) \
     (sizeof(T) == 8 ? PXB_STAGE_MIN_BLOCKS_F64 : ((AVG) ? PXB_STAGE_MIN_BLOCKS_AVG : PXB_STAGE_MIN_BLOCKS))
 
@@ -568,6 +576,7 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
         const int steady0 = min(L0 + 5, L1), steady1 = L1;
         int r = L0;
         for (; r < steady0; ++r) iterate(r, std::false_type{});
+        PXB_UNROLL(PXB_STAGE_UNROLL)
         for (; r < steady1; ++r) iterate(r, std::true_type{});
         for (; r < L1 + 5; ++r) iterate(r, std::false_type{});
         cp_async_wait<0>();  // the buffers are reused by the next item
