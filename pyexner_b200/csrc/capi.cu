@@ -299,9 +299,10 @@ struct Geometry {
     int band_rows = 0, nstrips = 0, nbands = 0, grid = 0;
 };
 
-Geometry stage_geometry(int ny, int nx, int resident_warps, int want_rows) {
+Geometry stage_geometry(int ny, int nx, int esize, int resident_warps, int want_rows) {
     Geometry g;
-    g.nstrips = std::max(1, (nx - 3 + PXB_STRIP_OUT - 1) / PXB_STRIP_OUT);
+    const int sout = pxb_stage_strip_out(esize);
+    g.nstrips = std::max(1, (nx - 3 + sout - 1) / sout);
     int rows = want_rows;
     if (rows <= 0) {
         // enough bands to give every resident warp an item, but no band taller than 128
@@ -909,7 +910,7 @@ int re_autotune_impl(pxb_re_plan* P, const pxb_re_fields* A, const pxb_re_fields
             const bool mpm = v & 4, hm = v & 2, avg = v & 1;
             const int bps = f64 ? pxb::re_stage_blocks_per_sm<double>(mpm, hm, avg)
                                 : pxb::re_stage_blocks_per_sm<float>(mpm, hm, avg);
-            P->stage[v] = stage_geometry(P->c.ny, P->c.nx, std::max(1, bps) * 4 * P->c.sm_count, rows);
+            P->stage[v] = stage_geometry(P->c.ny, P->c.nx, f64 ? 8 : 4, std::max(1, bps) * 4 * P->c.sm_count, rows);
         }
     };
     set_rows(0);
@@ -1133,7 +1134,8 @@ pxb::REStageArgs<T> ens_stage_args(const pxb_re_ens* E, int k, const pxb_re_fiel
     a.ring = mb.ring;
     a.sed = ens_sed<T>(E);
     a.band_rows = E->band_rows;
-    a.nstrips = std::max(1, (mb.nx - 3 + PXB_STRIP_OUT - 1) / PXB_STRIP_OUT);
+    const int sout = pxb_stage_strip_out((int)sizeof(T));
+    a.nstrips = std::max(1, (mb.nx - 3 + sout - 1) / sout);
     a.nbands = std::max(1, (mb.ny - 1 + E->band_rows - 1) / E->band_rows);
     a.err = &E->scr[k].err;
     return a;
@@ -1970,7 +1972,7 @@ int pxb_re_plan_create(const pxb_re_config* cfg, pxb_re_plan** out) {
         const bool mpm = v & 4, hm = v & 2, avg = v & 1;
         const int bps = f64 ? pxb::re_stage_blocks_per_sm<double>(mpm, hm, avg)
                             : pxb::re_stage_blocks_per_sm<float>(mpm, hm, avg);
-        P->stage[v] = stage_geometry(cfg->ny, cfg->nx, std::max(1, bps) * 4 * P->c.sm_count, cfg->band_rows);
+        P->stage[v] = stage_geometry(cfg->ny, cfg->nx, f64 ? 8 : 4, std::max(1, bps) * 4 * P->c.sm_count, cfg->band_rows);
     }
     const int cb = f64 ? pxb::re_cfl_blocks_per_sm<double>(cfg->nodata != nullptr)
                        : pxb::re_cfl_blocks_per_sm<float>(cfg->nodata != nullptr);

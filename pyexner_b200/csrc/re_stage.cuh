@@ -5,8 +5,9 @@
 // boundary handlers -> grass factor (:85-140) -> Exner update (:665-717) -> boundary
 // handlers, and for the second SSPRK2 stage the 0.5/0.5 combination (SSPRK2.py:40).
 //
-// Layout of the work: a warp owns a strip of 32 columns (3 halo | 26 owned | 3 halo) and
-// marches down a band of rows.  Each iteration consumes one new row, copied into the
+// Layout of the work: a warp owns a strip of 32 x CPT columns (3 halo | owned | 3 halo;
+// CPT = 2 consecutive columns per lane in float32, 1 in float64) and marches down a band
+// of rows.  Each iteration consumes one new row, copied into the
 // warp's shared buffer by cp.async during the previous iteration (together with the
 // partner-state values the averaging stage stores in this one), and advances a software
 // pipeline held in registers:
@@ -25,16 +26,17 @@
 
 #include "pxb_device.cuh"
 
-// Resident 128-thread blocks per SM the build is register-limited to (tuning knobs,
-// measured on the 2048^2 and 8192^2 Gaussian-bed cases): 4 (128 registers, no spills)
-// for both the plain stage and the averaging second SSPRK2 stage; 5 (96 registers) is
-// 1% faster at 8192^2 and 4% slower at 2048^2, where fewer resident warps mean taller
-// bands and fewer redundant halo rows.
+// Resident 128-thread blocks per SM the float32 build is register-limited to, for the
+// plain stage and the averaging second SSPRK2 stage (tuning knobs, measured on the
+// 2048^2 and 8192^2 Gaussian-bed cases): 4 (128 registers, no spills) with one column
+// per lane; 5 (96 registers) is 1% faster at 8192^2 and 4% slower at 2048^2, where fewer
+// resident warps mean taller bands and fewer redundant halo rows.  With two columns per
+// lane the state needs about 200 registers: 3 blocks (168, some spills) or 2.
 #ifndef PXB_STAGE_MIN_BLOCKS
-#define PXB_STAGE_MIN_BLOCKS 4
+#define PXB_STAGE_MIN_BLOCKS (PXB_STAGE_CPT_F32 == 2 ? 3 : 4)
 #endif
 #ifndef PXB_STAGE_MIN_BLOCKS_AVG
-#define PXB_STAGE_MIN_BLOCKS_AVG 4
+#define PXB_STAGE_MIN_BLOCKS_AVG (PXB_STAGE_CPT_F32 == 2 ? 3 : 4)
 #endif
 // float64 state (twice the registers per value)
 #ifndef PXB_STAGE_MIN_BLOCKS_F64
@@ -123,10 +125,71 @@ __device__ __forceinline__ ECell<T> shfl_down_ecell(const ECell<T>& p) {
     return q;
 }
 
+// Donor values of the boundary passes for the CPT columns of this lane: column k takes
+// the value at (row q+dy[k], column +dxo[k]) with dy, dxo in [-1, 1].  The candidates
+// are this lane's own columns and the last column of the west lane / first column of
+// the east lane (one shuffle each); the row is chosen by the receiver.  Donors lie in
+// another row only for cells of the first and last rows (plan creation checks it), so
+// elsewhere (dyrow false) only the middle row is fetched.
+template <int CPT, class T>
+__device__ __forceinline__ T pick_col(const T (&cand)[CPT + 2], int s) {
+    T v = cand[0];
+#pragma unroll
+    for (int t = 1; t < CPT + 2; ++t) v = (s == t) ? cand[t] : v;
+    return v;
+}
+
+template <int CPT, class T>
+__device__ __forceinline__ void donor_candidates(const T (&x)[CPT], T (&cd)[CPT + 2]) {
+    cd[0] = __shfl_up_sync(FULL, x[CPT - 1], 1);
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) cd[k + 1] = x[k];
+    cd[CPT + 1] = __shfl_down_sync(FULL, x[0], 1);
+}
+
+template <int CPT, class T>
+__device__ __forceinline__ void fetch_donor(bool dyrow, const int (&dy)[CPT], const int (&dxo)[CPT],
+                                            const T (&above)[CPT], const T (&mid)[CPT], const T (&below)[CPT],
+                                            T (&out)[CPT]) {
+    T cm[CPT + 2];
+    donor_candidates<CPT>(mid, cm);
+    if (!dyrow) {
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) out[k] = pick_col<CPT>(cm, k + dxo[k] + 1);
+        return;
+    }
+    T ca[CPT + 2], cbl[CPT + 2];
+    donor_candidates<CPT>(above, ca);
+    donor_candidates<CPT>(below, cbl);
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+        const int s = k + dxo[k] + 1;
+        out[k] = pick_row(dy[k], pick_col<CPT>(ca, s), pick_col<CPT>(cm, s), pick_col<CPT>(cbl, s));
+    }
+}
+
+// CPT consecutive elements of a shared row buffer laid out by column (lane * CPT + k).
+template <int CPT, class T>
+__device__ __forceinline__ void read_cols(const T* rowp, int lane, T (&v)[CPT]) {
+    if constexpr (CPT == 2 && sizeof(T) == 4) {
+        const float2 t = *reinterpret_cast<const float2*>(rowp + 2 * lane);
+        v[0] = t.x;
+        v[1] = t.y;
+    } else {
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) v[k] = rowp[CPT * lane + k];
+    }
+}
+
 // One work item (a strip of one band) of a stage; the single-grid kernel and the
-// ensemble kernel (ens_stage.cuh) both loop over items and call this.
+// ensemble kernel (ens.cuh) both loop over items and call this.  Each lane owns CPT
+// consecutive columns (pxb_stage_cpt): a strip is 32 * CPT columns, 3 halo | owned | 3
+// halo.  Neighbour values inside a lane are plain registers; across lanes one shuffle
+// moves the first (east) or last (west) column.
 template <class T, bool MPM, bool HAS_MASK, bool AVG>
 __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int item, bool& bad) {
+    constexpr int CPT = pxb_stage_cpt((int)sizeof(T));
+    constexpr int W = 32 * CPT;
     const int lane = threadIdx.x & 31;
     const int ny = a.ny, nx = a.nx;
     const unsigned upitch = (unsigned)a.pitch;  // planes are < 2^31 elements (checked at plan creation)
@@ -137,17 +200,22 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
     {
         const int ipb = pxb_stage_items_per_band(a.nstrips);
         const int band = item / ipb;
-        const int k = item - band * ipb;
-        int strip = k - 1, half = -1;  // half: 0 / 1 = upper / lower half of a boundary strip
+        const int kb = item - band * ipb;
+        int strip = kb - 1, half = -1;  // half: 0 / 1 = upper / lower half of a boundary strip
         if (ipb == 1) strip = 0;
-        else if (k < 2) { strip = 0; half = k; }
-        else if (k >= a.nstrips) { strip = a.nstrips - 1; half = k - a.nstrips; }
-        const int c = strip * PXB_STRIP_OUT - PXB_HALO + lane;
-        const bool colok = (c >= 0) && (c < nx);
-        const bool has_e = colok && (c + 1 < nx) && (lane < 31);
+        else if (kb < 2) { strip = 0; half = kb; }
+        else if (kb >= a.nstrips) { strip = a.nstrips - 1; half = kb - a.nstrips; }
         const bool last_strip = strip == a.nstrips - 1;
-        const bool out_col = colok && lane >= PXB_HALO && (lane < PXB_HALO + PXB_STRIP_OUT || last_strip);
-        const bool interior_col = (c >= 1) && (c <= nx - 2);
+        const int cb = strip * (W - 2 * PXB_HALO) - PXB_HALO + CPT * lane;  // column of this lane's first element
+        bool colok[CPT], has_e[CPT], out_col[CPT], interior_col[CPT];
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+            const int c = cb + k, j = CPT * lane + k;
+            colok[k] = (c >= 0) && (c < nx);
+            has_e[k] = colok[k] && (c + 1 < nx) && (j < W - 1);
+            out_col[k] = colok[k] && j >= PXB_HALO && (j < W - PXB_HALO || last_strip);
+            interior_col[k] = (c >= 1) && (c <= nx - 2);
+        }
         const int B0 = band * a.band_rows;
         const int B1 = (band == a.nbands - 1) ? ny : B0 + a.band_rows;
         const int Bm = B0 + (B1 - B0 + 1) / 2;
@@ -158,18 +226,33 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
         const bool bc_strip = (a.ring != nullptr) && (strip == 0 || last_strip);
         const bool bc_rows = (a.ring != nullptr) && (R0 == 0 || R1 == ny);
 
-        // ---- carried pipeline state
-        HCell<T> pA = make_hcell(T(0), T(0), T(0), T(0), T(0), T(0));
-        T hA = 0, huA = 0, hvA = 0, ztA = 0;
-        T xfA0 = 0, xfA1 = 0, xfA2 = 0, nfA0 = 0, nfA1 = 0, nfA2 = 0;
-        T hr3 = 0, hr2 = 0, hur2 = 0, hvr2 = 0, zt3 = 0, zt2 = 0;
-        unsigned mwin = 0;  // bit k = nodata of row r-1-k
-        T zin1 = 0, zin2 = 0, zin3 = 0, zin4 = 0;
-        T gin1 = 0, gin2 = 0, gin3 = 0, gin4 = 0;
-        T hf4h = 0, hf4u = 0, hf4v = 0, hf3h = 0, hf3u = 0, hf3v = 0;
-        ECell<T> e4 = make_ecell(T(0), T(0), T(0), T(0), T(0));
-        T xe4 = 0, fn4 = 0;
-        T zbp6 = 0, zbp5 = 0, gg6 = 0, gg5 = 0;
+        // ---- carried pipeline state, per column
+        HCell<T> pA[CPT];
+        T hA[CPT], huA[CPT], hvA[CPT], ztA[CPT];
+        T xfA[CPT][3], nfA[CPT][3];
+        T hr3[CPT], hr2[CPT], hur2[CPT], hvr2[CPT], zt3[CPT], zt2[CPT];
+        unsigned mwin[CPT];  // bit i = nodata of row r-1-i
+        T zin1[CPT], zin2[CPT], zin3[CPT], zin4[CPT];
+        T gin1[CPT], gin2[CPT], gin3[CPT], gin4[CPT];
+        T hf4h[CPT], hf4u[CPT], hf4v[CPT], hf3h[CPT], hf3u[CPT], hf3v[CPT];
+        ECell<T> e4[CPT];
+        T xe4[CPT], fn4[CPT];
+        T zbp6[CPT], zbp5[CPT], gg6[CPT], gg5[CPT];
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+            pA[k] = make_hcell(T(0), T(0), T(0), T(0), T(0), T(0));
+            hA[k] = huA[k] = hvA[k] = ztA[k] = T(0);
+#pragma unroll
+            for (int m = 0; m < 3; ++m) xfA[k][m] = nfA[k][m] = T(0);
+            hr3[k] = hr2[k] = hur2[k] = hvr2[k] = zt3[k] = zt2[k] = T(0);
+            mwin[k] = 0u;
+            zin1[k] = zin2[k] = zin3[k] = zin4[k] = T(0);
+            gin1[k] = gin2[k] = gin3[k] = gin4[k] = T(0);
+            hf4h[k] = hf4u[k] = hf4v[k] = hf3h[k] = hf3u[k] = hf3v[k] = T(0);
+            e4[k] = make_ecell(T(0), T(0), T(0), T(0), T(0));
+            xe4[k] = fn4[k] = T(0);
+            zbp6[k] = zbp5[k] = gg6[k] = gg5[k] = T(0);
+        }
 
         // Row r+1 is fetched while row r is computed: the loads of one iteration are in
         // flight during the ~thousand instructions of the previous one.  In float32 they
@@ -177,42 +260,51 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
         // float64 (measured: faster there) plain loads into registers.
         constexpr bool ASYNC_ROWS = is_f32<T>();
         constexpr int NP = MPM ? 6 : 7;
-        __shared__ T rbuf[4][ASYNC_ROWS ? 2 : 1][ASYNC_ROWS ? NP : 1][32];
-        T(*rb)[ASYNC_ROWS ? NP : 1][32] = rbuf[threadIdx.x >> 5];
-        T nh = 0, nhu = 0, nhv = 0, nzb = 0, nz = 0, nnb = 0, ng = 0;
-        bool nm = false;
-        auto load_row = [&](int rr) {
-            const int b = rr & 1;
-            if constexpr (!ASYNC_ROWS) {
-                if (rr < L1 && colok) {
-                    const unsigned i = (unsigned)rr * upitch + (unsigned)c;
-                    nh = __ldg(a.h + i);
-                    nhu = __ldg(a.hu + i);
-                    nhv = __ldg(a.hv + i);
-                    nzb = __ldg(a.zb + i);
-                    nz = __ldg(a.z + i);
-                    nnb = __ldg(a.nb + i);
-                    if (!MPM) ng = __ldg(a.G + i);
-                    if (HAS_MASK) nm = __ldg(a.nodata + i) != 0;
-                } else {
-                    nh = nhu = nhv = nzb = nz = nnb = ng = T(0);
-                    nm = false;
-                }
-            } else {
-                if (rr < L1 && colok) {
-                    const unsigned i = (unsigned)rr * upitch + (unsigned)c;
-                    cp_async_elem(&rb[b][0][lane], a.h + i);
-                    cp_async_elem(&rb[b][1][lane], a.hu + i);
-                    cp_async_elem(&rb[b][2][lane], a.hv + i);
-                    cp_async_elem(&rb[b][3][lane], a.zb + i);
-                    cp_async_elem(&rb[b][4][lane], a.z + i);
-                    cp_async_elem(&rb[b][5][lane], a.nb + i);
-                    if constexpr (!MPM) cp_async_elem(&rb[b][NP - 1][lane], a.G + i);
-                    if (HAS_MASK) nm = __ldg(a.nodata + i) != 0;
-                } else {
+        __shared__ __align__(16) T rbuf[4][ASYNC_ROWS ? 2 : 1][ASYNC_ROWS ? NP : 1][ASYNC_ROWS ? W : 1];
+        T(*rb)[ASYNC_ROWS ? NP : 1][ASYNC_ROWS ? W : 1] = rbuf[threadIdx.x >> 5];
+        T nh[CPT], nhu[CPT], nhv[CPT], nzb[CPT], nz[CPT], nnb[CPT], ng[CPT];
+        bool nm[CPT];
 #pragma unroll
-                    for (int k = 0; k < NP; ++k) rb[b][k][lane] = T(0);
-                    nm = false;
+        for (int k = 0; k < CPT; ++k) {
+            nh[k] = nhu[k] = nhv[k] = nzb[k] = nz[k] = nnb[k] = ng[k] = T(0);
+            nm[k] = false;
+        }
+        auto load_row = [&](int rr) __attribute__((always_inline)) {
+            const int b = rr & 1;
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) {
+                const bool ok = rr < L1 && colok[k];
+                const unsigned i = (unsigned)rr * upitch + (unsigned)(cb + k);
+                if constexpr (!ASYNC_ROWS) {
+                    if (ok) {
+                        nh[k] = __ldg(a.h + i);
+                        nhu[k] = __ldg(a.hu + i);
+                        nhv[k] = __ldg(a.hv + i);
+                        nzb[k] = __ldg(a.zb + i);
+                        nz[k] = __ldg(a.z + i);
+                        nnb[k] = __ldg(a.nb + i);
+                        if (!MPM) ng[k] = __ldg(a.G + i);
+                        if (HAS_MASK) nm[k] = __ldg(a.nodata + i) != 0;
+                    } else {
+                        nh[k] = nhu[k] = nhv[k] = nzb[k] = nz[k] = nnb[k] = ng[k] = T(0);
+                        nm[k] = false;
+                    }
+                } else {
+                    const int e = CPT * lane + k;
+                    if (ok) {
+                        cp_async_elem(&rb[b][0][e], a.h + i);
+                        cp_async_elem(&rb[b][1][e], a.hu + i);
+                        cp_async_elem(&rb[b][2][e], a.hv + i);
+                        cp_async_elem(&rb[b][3][e], a.zb + i);
+                        cp_async_elem(&rb[b][4][e], a.z + i);
+                        cp_async_elem(&rb[b][5][e], a.nb + i);
+                        if constexpr (!MPM) cp_async_elem(&rb[b][NP - 1][e], a.G + i);
+                        if (HAS_MASK) nm[k] = __ldg(a.nodata + i) != 0;
+                    } else {
+#pragma unroll
+                        for (int pl = 0; pl < NP; ++pl) rb[b][pl][e] = T(0);
+                        nm[k] = false;
+                    }
                 }
             }
         };
@@ -225,164 +317,245 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
         // reads and then writes these cells, so both are safe when the output aliases the
         // partner.
         constexpr bool ASYNC_PARTNER = AVG && is_f32<T>();
-        __shared__ T pbuf[4][ASYNC_PARTNER ? 2 : 1][5][32];
-        T(*pb)[5][32] = pbuf[threadIdx.x >> 5];
-        auto partner_copy = [&](const int rr) {  // the rows stored in iteration rr
+        __shared__ __align__(16) T pbuf[4][ASYNC_PARTNER ? 2 : 1][5][ASYNC_PARTNER ? W : 1];
+        T(*pb)[5][ASYNC_PARTNER ? W : 1] = pbuf[threadIdx.x >> 5];
+        auto partner_copy = [&](const int rr) __attribute__((always_inline)) {  // the rows stored in iteration rr
             const int q0 = rr - 3, p0 = rr - 5;
             const int b = rr & 1;
-            if (q0 >= L0 && q0 < L1 && q0 >= R0 && q0 < R1 && out_col) {
-                const unsigned i = (unsigned)q0 * upitch + (unsigned)c;
-                cp_async_elem(&pb[b][0][lane], a.ah + i);
-                cp_async_elem(&pb[b][1][lane], a.ahu + i);
-                cp_async_elem(&pb[b][2][lane], a.ahv + i);
-            }
-            if (p0 >= L0 && p0 < L1 && p0 >= R0 && p0 < R1 && out_col) {
-                const unsigned i = (unsigned)p0 * upitch + (unsigned)c;
-                cp_async_elem(&pb[b][3][lane], a.azb + i);
-                if (a.oG) cp_async_elem(&pb[b][4][lane], a.aG + i);
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) {
+                const int e = CPT * lane + k;
+                if (q0 >= L0 && q0 < L1 && q0 >= R0 && q0 < R1 && out_col[k]) {
+                    const unsigned i = (unsigned)q0 * upitch + (unsigned)(cb + k);
+                    cp_async_elem(&pb[b][0][e], a.ah + i);
+                    cp_async_elem(&pb[b][1][e], a.ahu + i);
+                    cp_async_elem(&pb[b][2][e], a.ahv + i);
+                }
+                if (p0 >= L0 && p0 < L1 && p0 >= R0 && p0 < R1 && out_col[k]) {
+                    const unsigned i = (unsigned)p0 * upitch + (unsigned)(cb + k);
+                    cp_async_elem(&pb[b][3][e], a.azb + i);
+                    if (a.oG) cp_async_elem(&pb[b][4][e], a.aG + i);
+                }
             }
         };
-        if (ASYNC_PARTNER) partner_copy(L0);
+        if constexpr (ASYNC_PARTNER) partner_copy(L0);
         cp_async_commit();
-        // Boundary recipes (first / last strip, first / last row): the recipe of the row
-        // that the first boundary application treats in iteration r (q = r-3) is copied
-        // into this warp's shared buffer during iteration r-1, so no recipe load is waited
-        // on inside the pipeline; the first application leaves the z_b / G fields of the
+        // Boundary recipes of the side columns (first / last strip, rows other than the
+        // first and last): the recipe of the ring cell of the row that the first boundary
+        // application treats in iteration r (q = r-3) is copied into this warp's shared
+        // buffer during iteration r-1 (one slot per side), so no recipe load is waited on
+        // inside the pipeline; the first and last rows, where every column is a ring cell,
+        // read theirs directly.  The first application leaves the z_b / G fields of the
         // second (row p = r-5, two iterations later) in a packed word.  Float32 only, as
         // the row copies.
         constexpr bool ASYNC_RECIPES = ASYNC_ROWS;
-        __shared__ __align__(16) pxb_ring_recipe rcbuf[4][ASYNC_RECIPES ? 2 : 1][32];
-        __shared__ unsigned zgbuf[4][ASYNC_RECIPES ? 4 : 1][32];
-        pxb_ring_recipe(*rcb)[32] = rcbuf[threadIdx.x >> 5];
-        unsigned(*zgb)[32] = zgbuf[threadIdx.x >> 5];
-        auto recipe_copy = [&](const int rr) {  // the recipes used in iteration rr
+        __shared__ __align__(16) pxb_ring_recipe rcbuf[4][ASYNC_RECIPES ? 2 : 1][2];
+        __shared__ unsigned zgbuf[4][ASYNC_RECIPES ? 4 : 1][ASYNC_RECIPES ? W : 1];
+        pxb_ring_recipe(*rcb)[2] = rcbuf[threadIdx.x >> 5];
+        unsigned(*zgb)[ASYNC_RECIPES ? W : 1] = zgbuf[threadIdx.x >> 5];
+        auto recipe_copy = [&](const int rr) __attribute__((always_inline)) {  // the recipes used in iteration rr
             const int qn = rr - 3;
-            if (qn >= L0 && qn < L1 && (bc_strip || (bc_rows && (qn == 0 || qn == ny - 1)))) {
-                const int slot = colok ? ring_slot(qn, c, ny, nx) : -1;
-                pxb_ring_recipe* d = &rcb[rr & 1][lane];
-                if (slot >= 0) {
-                    const char* src = reinterpret_cast<const char*>(a.ring + slot);
-                    char* dst = reinterpret_cast<char*>(d);
-                    cp_async16(dst, src);
-                    cp_async16(dst + 16, src + 16);
-                    cp_async16(dst + 32, src + 32);
-                } else {
-                    d->flags = 0u;
+            if (bc_strip && qn >= L0 && qn < L1 && qn != 0 && qn != ny - 1) {
+#pragma unroll
+                for (int k = 0; k < CPT; ++k) {
+                    const int c = cb + k;
+                    if (c == 0 || c == nx - 1) {
+                        const char* src = reinterpret_cast<const char*>(a.ring + ring_slot(qn, c, ny, nx));
+                        char* dst = reinterpret_cast<char*>(&rcb[rr & 1][c == 0 ? 0 : 1]);
+                        cp_async16(dst, src);
+                        cp_async16(dst + 16, src + 16);
+                        cp_async16(dst + 32, src + 32);
+                    }
                 }
             }
         };
 
         // One pipeline iteration.  In the steady state (rows L0+5 .. L1-1) every phase has
         // valid rows, so the row checks compile away.
-        auto iterate = [&](const int r, auto steady_tag) {
+        auto iterate = [&](const int r, auto steady_tag) __attribute__((always_inline)) {
             constexpr bool S = decltype(steady_tag)::value;
             const bool rowA = S || r < L1;
             // ================= A: row r (prefetched), x-faces of row r, y-face (r-1 | r)
-            T h_r, hu_r, hv_r, zb_r, z_r, nb_r, g_r = T(0);
+            T h_r[CPT], hu_r[CPT], hv_r[CPT], zb_r[CPT], z_r[CPT], nb_r[CPT], g_r[CPT];
             if constexpr (ASYNC_ROWS) {
                 cp_async_wait<0>();  // row r (and the partner rows stored in this iteration)
                 const int rbb = r & 1;
-                h_r = rb[rbb][0][lane];
-                hu_r = rb[rbb][1][lane];
-                hv_r = rb[rbb][2][lane];
-                zb_r = rb[rbb][3][lane];
-                z_r = rb[rbb][4][lane];
-                nb_r = rb[rbb][5][lane];
-                if constexpr (!MPM) g_r = rb[rbb][NP - 1][lane];
+                read_cols<CPT>(rb[rbb][0], lane, h_r);
+                read_cols<CPT>(rb[rbb][1], lane, hu_r);
+                read_cols<CPT>(rb[rbb][2], lane, hv_r);
+                read_cols<CPT>(rb[rbb][3], lane, zb_r);
+                read_cols<CPT>(rb[rbb][4], lane, z_r);
+                read_cols<CPT>(rb[rbb][5], lane, nb_r);
+                if constexpr (!MPM) {
+                    read_cols<CPT>(rb[rbb][NP - 1], lane, g_r);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < CPT; ++k) g_r[k] = T(0);
+                }
             } else {
-                h_r = nh, hu_r = nhu, hv_r = nhv, zb_r = nzb, z_r = nz, nb_r = nnb, g_r = ng;
+#pragma unroll
+                for (int k = 0; k < CPT; ++k) {
+                    h_r[k] = nh[k], hu_r[k] = nhu[k], hv_r[k] = nhv[k], zb_r[k] = nzb[k];
+                    z_r[k] = nz[k], nb_r[k] = nnb[k], g_r[k] = ng[k];
+                }
             }
-            const bool m_r = nm;
+            bool m_r[CPT];
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) m_r[k] = nm[k];
             load_row(r + 1);
-            if (ASYNC_PARTNER) partner_copy(r + 1);
-            if (ASYNC_RECIPES) recipe_copy(r + 1);
+            if constexpr (ASYNC_PARTNER) partner_copy(r + 1);
+            if constexpr (ASYNC_RECIPES) recipe_copy(r + 1);
             cp_async_commit();
-            T pah = 0, pahu = 0, pahv = 0, pazb = 0, paG = 0;
-            if (ASYNC_PARTNER) {
-                // read at the stores below
-            } else if (AVG) {
+            T pah[CPT], pahu[CPT], pahv[CPT], pazb[CPT], paG[CPT];
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) pah[k] = pahu[k] = pahv[k] = pazb[k] = paG[k] = T(0);
+            if constexpr (!ASYNC_PARTNER && AVG) {
                 const int q0 = r - 3, p0 = r - 5;
-                if ((S || (q0 >= L0 && q0 < L1)) && q0 >= R0 && q0 < R1 && out_col) {
-                    const unsigned i = (unsigned)q0 * upitch + (unsigned)c;
-                    pah = a.ah[i];
-                    pahu = a.ahu[i];
-                    pahv = a.ahv[i];
-                }
-                if ((S || (p0 >= L0 && p0 < L1)) && p0 >= R0 && p0 < R1 && out_col) {
-                    const unsigned i = (unsigned)p0 * upitch + (unsigned)c;
-                    pazb = a.azb[i];
-                    if (a.oG) paG = a.aG[i];
+#pragma unroll
+                for (int k = 0; k < CPT; ++k) {
+                    if ((S || (q0 >= L0 && q0 < L1)) && q0 >= R0 && q0 < R1 && out_col[k]) {
+                        const unsigned i = (unsigned)q0 * upitch + (unsigned)(cb + k);
+                        pah[k] = a.ah[i];
+                        pahu[k] = a.ahu[i];
+                        pahv[k] = a.ahv[i];
+                    }
+                    if ((S || (p0 >= L0 && p0 < L1)) && p0 >= R0 && p0 < R1 && out_col[k]) {
+                        const unsigned i = (unsigned)p0 * upitch + (unsigned)(cb + k);
+                        pazb[k] = a.azb[i];
+                        if (a.oG) paG[k] = a.aG[i];
+                    }
                 }
             }
-            const HCell<T> pr = make_hcell(h_r, hu_r, hv_r, zb_r, z_r, nb_r);
-            const T zt_r = z_r + zb_r;
-            T xf0 = 0, xf1 = 0, xf2 = 0;
+            HCell<T> pr[CPT];
+            T zt_r[CPT];
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) {
+                pr[k] = make_hcell(h_r[k], hu_r[k], hv_r[k], zb_r[k], z_r[k], nb_r[k]);
+                zt_r[k] = z_r[k] + zb_r[k];
+            }
+            T xf[CPT][3];
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) xf[k][0] = xf[k][1] = xf[k][2] = T(0);
             // In the prologue / drain iterations of a band the faces of invalid rows are
             // skipped for the whole warp (r is warp-uniform); their results would be masked.
             if (S || rowA) {
-                const HCell<T> pe = shfl_down_hcell(pr);
-                const T he = __shfl_down_sync(FULL, h_r, 1);
-                const bool me = HAS_MASK ? (__shfl_down_sync(FULL, (int)m_r, 1) != 0) : false;
-                const bool xact = rowA && has_e && ((h_r > DRY) || (he > DRY)) && !(m_r || me);
-                T P[3], M[3];
-                roe_exner_face<T, false>(pr, pe, dx, P, M);
+                HCell<T> pe[CPT];
+                T he[CPT];
+                bool me[CPT];
 #pragma unroll
-                for (int k = 0; k < 3; ++k) { P[k] = xact ? P[k] : T(0); M[k] = xact ? M[k] : T(0); }
-                const T w0 = __shfl_up_sync(FULL, P[0], 1);
-                const T w1 = __shfl_up_sync(FULL, P[1], 1);
-                const T w2 = __shfl_up_sync(FULL, P[2], 1);
-                const bool wact = (__shfl_up_sync(FULL, (int)xact, 1) != 0) && lane > 0;
+                for (int k = 0; k + 1 < CPT; ++k) { pe[k] = pr[k + 1]; he[k] = h_r[k + 1]; me[k] = m_r[k + 1]; }
+                pe[CPT - 1] = shfl_down_hcell(pr[0]);
+                he[CPT - 1] = __shfl_down_sync(FULL, h_r[0], 1);
+                me[CPT - 1] = HAS_MASK ? (__shfl_down_sync(FULL, (int)m_r[0], 1) != 0) : false;
+                T P[CPT][3], M[CPT][3];
+                bool xact[CPT];
+#pragma unroll
+                for (int k = 0; k < CPT; ++k) {
+                    xact[k] = rowA && has_e[k] && ((h_r[k] > DRY) || (he[k] > DRY)) && !(m_r[k] || me[k]);
+                    roe_exner_face<T, false>(pr[k], pe[k], dx, P[k], M[k]);
+#pragma unroll
+                    for (int m = 0; m < 3; ++m) {
+                        P[k][m] = xact[k] ? P[k][m] : T(0);
+                        M[k][m] = xact[k] ? M[k][m] : T(0);
+                    }
+                }
+                // upwP of the west face of column k: own column k-1, or the west lane's last
+                T wP[CPT][3];
+                bool wact[CPT];
+#pragma unroll
+                for (int k = 1; k < CPT; ++k) {
+                    wact[k] = xact[k - 1];
+#pragma unroll
+                    for (int m = 0; m < 3; ++m) wP[k][m] = P[k - 1][m];
+                }
+#pragma unroll
+                for (int m = 0; m < 3; ++m) wP[0][m] = __shfl_up_sync(FULL, P[CPT - 1][m], 1);
+                wact[0] = (__shfl_up_sync(FULL, (int)xact[CPT - 1], 1) != 0) && lane > 0;
                 // scatter order of roe_exner.py:599-600: east upwM first, then west upwP
-                if (xact) { xf0 = xf0 + M[0]; xf1 = xf1 + M[1]; xf2 = xf2 + M[2]; }
-                if (wact) { xf0 = xf0 + w0; xf1 = xf1 + w1; xf2 = xf2 + w2; }
-            }
-            T yP[3] = {T(0), T(0), T(0)}, yM[3] = {T(0), T(0), T(0)};
-            const bool yact = rowA && (S || r - 1 >= L0) && colok && ((hA > DRY) || (h_r > DRY)) && !((mwin & 1u) || m_r);
-            if (S || (rowA && r - 1 >= L0)) {
-                roe_exner_face<T, true>(pA, pr, dx, yP, yM);
 #pragma unroll
-                for (int k = 0; k < 3; ++k) { yP[k] = yact ? yP[k] : T(0); yM[k] = yact ? yM[k] : T(0); }
+                for (int k = 0; k < CPT; ++k) {
+#pragma unroll
+                    for (int m = 0; m < 3; ++m) {
+                        if (xact[k]) xf[k][m] = xf[k][m] + M[k][m];
+                        if (wact[k]) xf[k][m] = xf[k][m] + wP[k][m];
+                    }
+                }
+            }
+            T yP[CPT][3], yM[CPT][3];
+#pragma unroll
+            for (int k = 0; k < CPT; ++k)
+#pragma unroll
+                for (int m = 0; m < 3; ++m) yP[k][m] = yM[k][m] = T(0);
+            if (S || (rowA && r - 1 >= L0)) {
+#pragma unroll
+                for (int k = 0; k < CPT; ++k) {
+                    const bool yact = rowA && (S || r - 1 >= L0) && colok[k] && ((hA[k] > DRY) || (h_r[k] > DRY)) &&
+                                      !((mwin[k] & 1u) || m_r[k]);
+                    roe_exner_face<T, true>(pA[k], pr[k], dx, yP[k], yM[k]);
+#pragma unroll
+                    for (int m = 0; m < 3; ++m) {
+                        yP[k][m] = yact ? yP[k][m] : T(0);
+                        yM[k][m] = yact ? yM[k][m] : T(0);
+                    }
+                }
             }
 
             // ================= B: hydro update of row r-1
-            T hr1 = 0, hur1 = 0, hvr1 = 0;
-            if (S || (r - 1 >= L0 && r - 1 < L1)) {
-                T f0 = xfA0, f1 = xfA1, f2 = xfA2;
-                f0 = f0 + yM[0]; f1 = f1 + yM[1]; f2 = f2 + yM[2];      // south face upwM
-                f0 = f0 + nfA0; f1 = f1 + nfA1; f2 = f2 + nfA2;         // north face upwP
-                if constexpr (is_f32<T>()) {
-                    hr1 = hA - dtdx * f0;
-                    hur1 = huA - dtdx * f1;
-                    hvr1 = hvA - dtdx * f2;
-                } else {
-                    hr1 = hA - dt * f0 / dx;
-                    hur1 = huA - dt * f1 / dx;
-                    hvr1 = hvA - dt * f2 / dx;
+            T hr1[CPT], hur1[CPT], hvr1[CPT];
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) {
+                hr1[k] = hur1[k] = hvr1[k] = T(0);
+                if (S || (r - 1 >= L0 && r - 1 < L1)) {
+                    T f0 = xfA[k][0], f1 = xfA[k][1], f2 = xfA[k][2];
+                    f0 = f0 + yM[k][0]; f1 = f1 + yM[k][1]; f2 = f2 + yM[k][2];    // south face upwM
+                    f0 = f0 + nfA[k][0]; f1 = f1 + nfA[k][1]; f2 = f2 + nfA[k][2];  // north face upwP
+                    if constexpr (is_f32<T>()) {
+                        hr1[k] = hA[k] - dtdx * f0;
+                        hur1[k] = huA[k] - dtdx * f1;
+                        hvr1[k] = hvA[k] - dtdx * f2;
+                    } else {
+                        hr1[k] = hA[k] - dt * f0 / dx;
+                        hur1[k] = huA[k] - dt * f1 / dx;
+                        hvr1[k] = hvA[k] - dt * f2 / dx;
+                    }
                 }
             }
 
             // ================= C: momentum corrections of row r-2
-            T hf2h = 0, hf2u = 0, hf2v = 0;
+            T hf2h[CPT], hf2u[CPT], hf2v[CPT];
             {
                 const int q2 = r - 2;
-                const T hE = __shfl_down_sync(FULL, hr2, 1), hW = __shfl_up_sync(FULL, hr2, 1);
-                const T zE = __shfl_down_sync(FULL, zt2, 1), zW = __shfl_up_sync(FULL, zt2, 1);
-                const bool m2 = HAS_MASK && ((mwin >> 1) & 1u);
-                const bool mE = HAS_MASK ? (__shfl_down_sync(FULL, (int)m2, 1) != 0) : false;
-                const bool mW = HAS_MASK ? (__shfl_up_sync(FULL, (int)m2, 1) != 0) : false;
-                if (S || (q2 >= L0 && q2 < L1)) {
-                    hf2h = hr2;
-                    hf2u = hur2;
-                    hf2v = hvr2;
-                    if (interior_col && q2 >= 1 && q2 <= ny - 2) {
-                        const bool mN = HAS_MASK && ((mwin >> 2) & 1u);
-                        const bool mS = HAS_MASK && (mwin & 1u);
-                        const T eta = hr2 + zt2;
-                        const bool stop_u = ((eta < zE) && (hE < DRY)) || ((eta < zW) && (hW < DRY)) || mE || mW;
-                        const bool stop_v = ((eta < zt3) && (hr3 < DRY)) || ((eta < ztA) && (hr1 < DRY)) || mN || mS;
-                        const bool active = (hr2 > DRY) && !m2;
-                        hf2u = (active && !stop_u) ? hur2 : T(0);
-                        hf2v = (active && !stop_v) ? hvr2 : T(0);
+                T hE[CPT], hW[CPT], zE[CPT], zW[CPT];
+                bool m2[CPT], mE[CPT], mW[CPT];
+#pragma unroll
+                for (int k = 0; k < CPT; ++k) m2[k] = HAS_MASK && ((mwin[k] >> 1) & 1u);
+#pragma unroll
+                for (int k = 0; k + 1 < CPT; ++k) { hE[k] = hr2[k + 1]; zE[k] = zt2[k + 1]; mE[k] = m2[k + 1]; }
+#pragma unroll
+                for (int k = 1; k < CPT; ++k) { hW[k] = hr2[k - 1]; zW[k] = zt2[k - 1]; mW[k] = m2[k - 1]; }
+                hE[CPT - 1] = __shfl_down_sync(FULL, hr2[0], 1);
+                zE[CPT - 1] = __shfl_down_sync(FULL, zt2[0], 1);
+                hW[0] = __shfl_up_sync(FULL, hr2[CPT - 1], 1);
+                zW[0] = __shfl_up_sync(FULL, zt2[CPT - 1], 1);
+                mE[CPT - 1] = HAS_MASK ? (__shfl_down_sync(FULL, (int)m2[0], 1) != 0) : false;
+                mW[0] = HAS_MASK ? (__shfl_up_sync(FULL, (int)m2[CPT - 1], 1) != 0) : false;
+#pragma unroll
+                for (int k = 0; k < CPT; ++k) {
+                    hf2h[k] = hf2u[k] = hf2v[k] = T(0);
+                    if (S || (q2 >= L0 && q2 < L1)) {
+                        hf2h[k] = hr2[k];
+                        hf2u[k] = hur2[k];
+                        hf2v[k] = hvr2[k];
+                        if (interior_col[k] && q2 >= 1 && q2 <= ny - 2) {
+                            const bool mN = HAS_MASK && ((mwin[k] >> 2) & 1u);
+                            const bool mS = HAS_MASK && (mwin[k] & 1u);
+                            const T eta = hr2[k] + zt2[k];
+                            const bool stop_u = ((eta < zE[k]) && (hE[k] < DRY)) || ((eta < zW[k]) && (hW[k] < DRY)) || mE[k] || mW[k];
+                            const bool stop_v = ((eta < zt3[k]) && (hr3[k] < DRY)) || ((eta < ztA[k]) && (hr1[k] < DRY)) || mN || mS;
+                            const bool active = (hr2[k] > DRY) && !m2[k];
+                            hf2u[k] = (active && !stop_u) ? hur2[k] : T(0);
+                            hf2v[k] = (active && !stop_v) ? hvr2[k] : T(0);
+                        }
                     }
                 }
             }
@@ -394,184 +567,256 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
             // a hydro boundary cell (checked at plan creation), so its value is HF.
             const int q = r - 3;
             const bool rowD = S || ((q >= L0) && (q < L1));
-            T hbh = hf3h, hbu = hf3u, hbv = hf3v, zb1 = zin3, gb1 = gin3;
-            T sbh = hf3h, sbu = hf3u, sbv = hf3v;
+            T hbh[CPT], hbu[CPT], hbv[CPT], zb1[CPT], gb1[CPT], sbh[CPT], sbu[CPT], sbv[CPT];
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) {
+                hbh[k] = sbh[k] = hf3h[k];
+                hbu[k] = sbu[k] = hf3u[k];
+                hbv[k] = sbv[k] = hf3v[k];
+                zb1[k] = zin3[k];
+                gb1[k] = gin3[k];
+            }
             if (rowD && (bc_strip || (bc_rows && (q == 0 || q == ny - 1)))) {
-                unsigned flags = 0;
-                int hdy = 0, hdx = 0, mdy = 0, mdx = 0, zdy = 0, zdx = 0, gdy = 0, gdx = 0;
-                T m0 = 0, m1 = 0, m2c = 0, m3 = 0;
-                auto take = [&](const pxb_ring_recipe& rc) {
-                    flags = rc.flags;
-                    hdy = rc.h_dy; hdx = rc.h_dx; mdy = rc.m_dy; mdx = rc.m_dx;
-                    zdy = rc.zb_dy; zdx = rc.zb_dx; gdy = rc.g_dy; gdx = rc.g_dx;
-                    m0 = T(rc.m[0]); m1 = T(rc.m[1]); m2c = T(rc.m[2]); m3 = T(rc.m[3]);
-                };
-                if constexpr (ASYNC_RECIPES) {
-                    const pxb_ring_recipe& rc = rcb[r & 1][lane];  // copied in iteration r-1
-                    if (rc.flags != 0u) take(rc);
-                    zgb[r & 3][lane] = pack_zg(flags, zdy, zdx, gdy, gdx);
-                } else {
-                    const int slot = colok ? ring_slot(q, c, ny, nx) : -1;
-                    if (slot >= 0) take(a.ring[slot]);
-                }
-                if (__any_sync(FULL, flags != 0)) {
-                    // Donor value at (row q+dy, column c+dx); the row is chosen by the
-                    // receiver.  Donors lie in another row only for cells of the first and
-                    // last rows (plan creation checks it), so other rows shuffle one value.
-                    const bool dyrow = (q == 0) || (q == ny - 1);
-                    auto fetch = [&](int dy, int dx_, T above, T mid, T below) {
-                        const T vm = __shfl_sync(FULL, mid, lane + dx_);
-                        if (!dyrow) return vm;
-                        const T va = __shfl_sync(FULL, above, lane + dx_);
-                        const T vb = __shfl_sync(FULL, below, lane + dx_);
-                        return pick_row(dy, va, vm, vb);
+                unsigned flags[CPT];
+                int hdy[CPT], hdx[CPT], mdy[CPT], mdx[CPT], zdy[CPT], zdx[CPT], gdy[CPT], gdx[CPT];
+                T m0[CPT], m1[CPT], m2c[CPT], m3[CPT];
+                bool anyf = false;
+#pragma unroll
+                for (int k = 0; k < CPT; ++k) {
+                    flags[k] = 0u;
+                    hdy[k] = hdx[k] = mdy[k] = mdx[k] = zdy[k] = zdx[k] = gdy[k] = gdx[k] = 0;
+                    m0[k] = m1[k] = m2c[k] = m3[k] = T(0);
+                    auto take = [&](const pxb_ring_recipe& rc) __attribute__((always_inline)) {
+                        flags[k] = rc.flags;
+                        hdy[k] = rc.h_dy; hdx[k] = rc.h_dx; mdy[k] = rc.m_dy; mdx[k] = rc.m_dx;
+                        zdy[k] = rc.zb_dy; zdx[k] = rc.zb_dx; gdy[k] = rc.g_dy; gdx[k] = rc.g_dx;
+                        m0[k] = T(rc.m[0]); m1[k] = T(rc.m[1]); m2c[k] = T(rc.m[2]); m3[k] = T(rc.m[3]);
                     };
-                    const T vh = fetch(hdy, hdx, hf4h, hf3h, hf2h);
-                    const T vu = fetch(mdy, mdx, hf4u, hf3u, hf2u);
-                    const T vv = fetch(mdy, mdx, hf4v, hf3v, hf2v);
-                    const T vz = fetch(zdy, zdx, zin4, zin3, zin2);
-                    if (flags & 1u) hbh = vh;
-                    if (flags & 2u) {
-                        if (flags & 4u) { hbu = m0; hbv = m1; }
-                        else { hbu = sum2(m0, vu, m1, vv); hbv = sum2(m2c, vu, m3, vv); }
+                    const int c = cb + k;
+                    bool direct = true;
+                    if constexpr (ASYNC_RECIPES) {
+                        if (q != 0 && q != ny - 1) {  // side rows: the ring column's recipe, copied in iteration r-1
+                            direct = false;
+                            if (c == 0 || c == nx - 1) take(rcb[r & 1][c == 0 ? 0 : 1]);
+                        }
                     }
-                    if (flags & 8u) zb1 = vz;
+                    if (direct) {
+                        const int slot = colok[k] ? ring_slot(q, c, ny, nx) : -1;
+                        if (slot >= 0) take(a.ring[slot]);
+                    }
+                    if constexpr (ASYNC_RECIPES) zgb[r & 3][CPT * lane + k] = pack_zg(flags[k], zdy[k], zdx[k], gdy[k], gdx[k]);
+                    anyf = anyf || (flags[k] != 0u);
+                }
+                if (__any_sync(FULL, anyf)) {
+                    const bool dyrow = (q == 0) || (q == ny - 1);
+                    T vh[CPT], vu[CPT], vv[CPT], vz[CPT];
+                    fetch_donor<CPT>(dyrow, hdy, hdx, hf4h, hf3h, hf2h, vh);
+                    fetch_donor<CPT>(dyrow, mdy, mdx, hf4u, hf3u, hf2u, vu);
+                    fetch_donor<CPT>(dyrow, mdy, mdx, hf4v, hf3v, hf2v, vv);
+                    fetch_donor<CPT>(dyrow, zdy, zdx, zin4, zin3, zin2, vz);
+#pragma unroll
+                    for (int k = 0; k < CPT; ++k) {
+                        if (flags[k] & 1u) hbh[k] = vh[k];
+                        if (flags[k] & 2u) {
+                            if (flags[k] & 4u) { hbu[k] = m0[k]; hbv[k] = m1[k]; }
+                            else { hbu[k] = sum2(m0[k], vu[k], m1[k], vv[k]); hbv[k] = sum2(m2c[k], vu[k], m3[k], vv[k]); }
+                        }
+                        if (flags[k] & 8u) zb1[k] = vz[k];
+                    }
                     if (!MPM) {
-                        const T vg = fetch(gdy, gdx, gin4, gin3, gin2);
-                        if (flags & 16u) gb1 = vg;
+                        T vg[CPT];
+                        fetch_donor<CPT>(dyrow, gdy, gdx, gin4, gin3, gin2, vg);
+#pragma unroll
+                        for (int k = 0; k < CPT; ++k)
+                            if (flags[k] & 16u) gb1[k] = vg[k];
                     }
                     // second pass
-                    const T wh = fetch(hdy, hdx, hf4h, hbh, hf2h);
-                    const T wu = fetch(mdy, mdx, hf4u, hbu, hf2u);
-                    const T wv = fetch(mdy, mdx, hf4v, hbv, hf2v);
-                    sbh = hbh;
-                    sbu = hbu;
-                    sbv = hbv;
-                    if (flags & 1u) sbh = wh;
-                    if ((flags & 2u) && !(flags & 4u)) {
-                        sbu = sum2(m0, wu, m1, wv);
-                        sbv = sum2(m2c, wu, m3, wv);
+                    T wh[CPT], wu[CPT], wv[CPT];
+                    fetch_donor<CPT>(dyrow, hdy, hdx, hf4h, hbh, hf2h, wh);
+                    fetch_donor<CPT>(dyrow, mdy, mdx, hf4u, hbu, hf2u, wu);
+                    fetch_donor<CPT>(dyrow, mdy, mdx, hf4v, hbv, hf2v, wv);
+#pragma unroll
+                    for (int k = 0; k < CPT; ++k) {
+                        sbh[k] = hbh[k];
+                        sbu[k] = hbu[k];
+                        sbv[k] = hbv[k];
+                        if (flags[k] & 1u) sbh[k] = wh[k];
+                        if ((flags[k] & 2u) && !(flags[k] & 4u)) {
+                            sbu[k] = sum2(m0[k], wu[k], m1[k], wv[k]);
+                            sbv[k] = sum2(m2c[k], wu[k], m3[k], wv[k]);
+                        }
                     }
                 }
             }
 
             // ================= E: grass factor, Exner cell and faces of row q
-            const bool mq = HAS_MASK && ((mwin >> 2) & 1u);
-            const bool mq1 = HAS_MASK && ((mwin >> 3) & 1u);
-            ECell<T> e3{};
-            T xe3 = 0, Fy = 0;
-            if (S || rowD) {  // warp-uniform: row q is outside the band's rows in some prologue / drain iterations
-            const T Gq = MPM ? mpm_grass(hbh, hbu, hbv, mq, a.sed) : const_grass(hbh, gb1, mq);
-            e3 = make_ecell(hbh, hbu, hbv, zb1, Gq);
-            {
-                const ECell<T> ee = shfl_down_ecell(e3);
-                const bool mqe = HAS_MASK ? (__shfl_down_sync(FULL, (int)mq, 1) != 0) : false;
-                const bool xact = rowD && has_e && exner_active(e3, ee, mq, mqe);
-                const T Fx = exner_face<T, false>(e3, ee);
-                const T F = xact ? Fx : T(0);
-                const T Fw = __shfl_up_sync(FULL, F, 1);
-                const bool wact = (__shfl_up_sync(FULL, (int)xact, 1) != 0) && lane > 0;
-                // roe_exner.py:710-711: -F of the west face first, then +F of the east face
-                if (wact) xe3 = xe3 + (-Fw);
-                if (xact) xe3 = xe3 + F;
+            bool mq[CPT], mq1[CPT];
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) {
+                mq[k] = HAS_MASK && ((mwin[k] >> 2) & 1u);
+                mq1[k] = HAS_MASK && ((mwin[k] >> 3) & 1u);
             }
-            const bool yex = rowD && (S || q - 1 >= L0) && colok && exner_active(e4, e3, mq1, mq);
-            const T Fyv = exner_face<T, true>(e4, e3);
-            Fy = yex ? Fyv : T(0);
+            ECell<T> e3[CPT];
+            T xe3[CPT], Fy[CPT];
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) {
+                e3[k] = ECell<T>{};
+                xe3[k] = Fy[k] = T(0);
+            }
+            if (S || rowD) {  // warp-uniform: row q is outside the band's rows in some prologue / drain iterations
+#pragma unroll
+                for (int k = 0; k < CPT; ++k) {
+                    const T Gq = MPM ? mpm_grass(hbh[k], hbu[k], hbv[k], mq[k], a.sed) : const_grass(hbh[k], gb1[k], mq[k]);
+                    e3[k] = make_ecell(hbh[k], hbu[k], hbv[k], zb1[k], Gq);
+                }
+                ECell<T> ee[CPT];
+                bool mqe[CPT];
+#pragma unroll
+                for (int k = 0; k + 1 < CPT; ++k) { ee[k] = e3[k + 1]; mqe[k] = mq[k + 1]; }
+                ee[CPT - 1] = shfl_down_ecell(e3[0]);
+                mqe[CPT - 1] = HAS_MASK ? (__shfl_down_sync(FULL, (int)mq[0], 1) != 0) : false;
+                T F[CPT];
+                bool xact[CPT];
+#pragma unroll
+                for (int k = 0; k < CPT; ++k) {
+                    xact[k] = rowD && has_e[k] && exner_active(e3[k], ee[k], mq[k], mqe[k]);
+                    const T Fx = exner_face<T, false>(e3[k], ee[k]);
+                    F[k] = xact[k] ? Fx : T(0);
+                }
+                T Fw[CPT];
+                bool wact[CPT];
+#pragma unroll
+                for (int k = 1; k < CPT; ++k) { Fw[k] = F[k - 1]; wact[k] = xact[k - 1]; }
+                Fw[0] = __shfl_up_sync(FULL, F[CPT - 1], 1);
+                wact[0] = (__shfl_up_sync(FULL, (int)xact[CPT - 1], 1) != 0) && lane > 0;
+#pragma unroll
+                for (int k = 0; k < CPT; ++k) {
+                    // roe_exner.py:710-711: -F of the west face first, then +F of the east face
+                    if (wact[k]) xe3[k] = xe3[k] + (-Fw[k]);
+                    if (xact[k]) xe3[k] = xe3[k] + F[k];
+                    const bool yex = rowD && (S || q - 1 >= L0) && colok[k] && exner_active(e4[k], e3[k], mq1[k], mq[k]);
+                    const T Fyv = exner_face<T, true>(e4[k], e3[k]);
+                    Fy[k] = yex ? Fyv : T(0);
+                }
             }
 
             // ================= F: z_b update of row r-4
-            T zbp4 = 0;
-            if (S || (r - 4 >= L0 && r - 4 < L1)) {
-                T acc = xe4;
-                acc = acc + (-fn4);  // north face (roe_exner.py:712)
-                acc = acc + Fy;      // south face (roe_exner.py:713)
-                if constexpr (is_f32<T>()) zbp4 = e4.zb - dtdx * acc;
-                else zbp4 = e4.zb - dt * acc / dx;
+            T zbp4[CPT], gg4[CPT];
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) {
+                zbp4[k] = T(0);
+                if (S || (r - 4 >= L0 && r - 4 < L1)) {
+                    T acc = xe4[k];
+                    acc = acc + (-fn4[k]);  // north face (roe_exner.py:712)
+                    acc = acc + Fy[k];      // south face (roe_exner.py:713)
+                    if constexpr (is_f32<T>()) zbp4[k] = e4[k].zb - dtdx * acc;
+                    else zbp4[k] = e4[k].zb - dt * acc / dx;
+                }
+                gg4[k] = e4[k].G;
             }
-            const T gg4 = e4.G;
 
             // ================= G: second boundary application and stores of row p = r-5
             const int p = r - 5;
             const bool rowG = S || ((p >= L0) && (p < L1));
-            T zfin = zbp5, gfin = gg5;
+            T zfin[CPT], gfin[CPT];
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) { zfin[k] = zbp5[k]; gfin[k] = gg5[k]; }
             if (rowG && (bc_strip || (bc_rows && (p == 0 || p == ny - 1)))) {
-                unsigned flags = 0;
-                int zdy = 0, zdx = 0, gdy = 0, gdx = 0;
-                if constexpr (ASYNC_RECIPES) {
-                    const unsigned w = zgb[(r - 2) & 3][lane];  // left by the first application of row p
-                    flags = w & 24u;
-                    zdy = (int)((w >> 8) & 15u) - 8;
-                    zdx = (int)((w >> 12) & 15u) - 8;
-                    gdy = (int)((w >> 16) & 15u) - 8;
-                    gdx = (int)((w >> 20) & 15u) - 8;
-                } else {
-                    const int slot = colok ? ring_slot(p, c, ny, nx) : -1;
-                    if (slot >= 0) {
-                        const pxb_ring_recipe& rc = a.ring[slot];
-                        flags = rc.flags;
-                        zdy = rc.zb_dy; zdx = rc.zb_dx; gdy = rc.g_dy; gdx = rc.g_dx;
+                unsigned flags[CPT];
+                int zdy[CPT], zdx[CPT], gdy[CPT], gdx[CPT];
+                bool anyf = false;
+#pragma unroll
+                for (int k = 0; k < CPT; ++k) {
+                    flags[k] = 0u;
+                    zdy[k] = zdx[k] = gdy[k] = gdx[k] = 0;
+                    if constexpr (ASYNC_RECIPES) {
+                        const unsigned w = zgb[(r - 2) & 3][CPT * lane + k];  // left by the first application of row p
+                        flags[k] = w & 24u;
+                        zdy[k] = (int)((w >> 8) & 15u) - 8;
+                        zdx[k] = (int)((w >> 12) & 15u) - 8;
+                        gdy[k] = (int)((w >> 16) & 15u) - 8;
+                        gdx[k] = (int)((w >> 20) & 15u) - 8;
+                    } else {
+                        const int slot = colok[k] ? ring_slot(p, cb + k, ny, nx) : -1;
+                        if (slot >= 0) {
+                            const pxb_ring_recipe& rc = a.ring[slot];
+                            flags[k] = rc.flags;
+                            zdy[k] = rc.zb_dy; zdx[k] = rc.zb_dx; gdy[k] = rc.g_dy; gdx[k] = rc.g_dx;
+                        }
                     }
+                    anyf = anyf || ((flags[k] & 24u) != 0u);
                 }
-                if (__any_sync(FULL, (flags & 24u) != 0)) {
-                    T zv = __shfl_sync(FULL, zbp5, lane + zdx), gv = __shfl_sync(FULL, gg5, lane + gdx);
-                    if ((p == 0) || (p == ny - 1)) {  // donors in another row: first / last row only
-                        const T z6 = __shfl_sync(FULL, zbp6, lane + zdx), z4 = __shfl_sync(FULL, zbp4, lane + zdx);
-                        const T g6 = __shfl_sync(FULL, gg6, lane + gdx), g4 = __shfl_sync(FULL, gg4, lane + gdx);
-                        zv = pick_row(zdy, z6, zv, z4);
-                        gv = pick_row(gdy, g6, gv, g4);
+                if (__any_sync(FULL, anyf)) {
+                    const bool dyrow = (p == 0) || (p == ny - 1);
+                    T zv[CPT], gv[CPT];
+                    fetch_donor<CPT>(dyrow, zdy, zdx, zbp6, zbp5, zbp4, zv);
+                    fetch_donor<CPT>(dyrow, gdy, gdx, gg6, gg5, gg4, gv);
+#pragma unroll
+                    for (int k = 0; k < CPT; ++k) {
+                        if (flags[k] & 8u) zfin[k] = zv[k];
+                        if (flags[k] & 16u) gfin[k] = gv[k];
                     }
-                    if (flags & 8u) zfin = zv;
-                    if (flags & 16u) gfin = gv;
                 }
             }
-            if (rowG && p >= R0 && p < R1 && out_col) {
-                const unsigned i = (unsigned)p * upitch + (unsigned)c;
-                if (AVG) {
-                    if (ASYNC_PARTNER) {
-                        pazb = pb[r & 1][3][lane];
-                        if (a.oG) paG = pb[r & 1][4][lane];
-                    }
-                    zfin = T(0.5) * pazb + T(0.5) * zfin;
-                    if (a.oG) gfin = T(0.5) * paG + T(0.5) * gfin;
+            if (rowG && p >= R0 && p < R1) {
+                if constexpr (ASYNC_PARTNER) {
+                    read_cols<CPT>(pb[r & 1][3], lane, pazb);
+                    if (a.oG) read_cols<CPT>(pb[r & 1][4], lane, paG);
                 }
-                a.ozb[i] = zfin;
-                if (a.oG) a.oG[i] = gfin;
-                bad |= !d_isfinite(zfin);
+#pragma unroll
+                for (int k = 0; k < CPT; ++k) {
+                    if (!out_col[k]) continue;
+                    const unsigned i = (unsigned)p * upitch + (unsigned)(cb + k);
+                    T zo = zfin[k], go = gfin[k];
+                    if (AVG) {
+                        zo = T(0.5) * pazb[k] + T(0.5) * zo;
+                        if (a.oG) go = T(0.5) * paG[k] + T(0.5) * go;
+                    }
+                    a.ozb[i] = zo;
+                    if (a.oG) a.oG[i] = go;
+                    bad |= !d_isfinite(zo);
+                }
             }
-            if (rowD && q >= R0 && q < R1 && out_col) {
-                const unsigned i = (unsigned)q * upitch + (unsigned)c;
-                T oh = sbh, ou = sbu, ov = sbv;
-                if (AVG) {
-                    if (ASYNC_PARTNER) {
-                        pah = pb[r & 1][0][lane];
-                        pahu = pb[r & 1][1][lane];
-                        pahv = pb[r & 1][2][lane];
-                    }
-                    oh = T(0.5) * pah + T(0.5) * oh;
-                    ou = T(0.5) * pahu + T(0.5) * ou;
-                    ov = T(0.5) * pahv + T(0.5) * ov;
+            if (rowD && q >= R0 && q < R1) {
+                if constexpr (ASYNC_PARTNER) {
+                    read_cols<CPT>(pb[r & 1][0], lane, pah);
+                    read_cols<CPT>(pb[r & 1][1], lane, pahu);
+                    read_cols<CPT>(pb[r & 1][2], lane, pahv);
                 }
-                a.oh[i] = oh;
-                a.ohu[i] = ou;
-                a.ohv[i] = ov;
-                bad |= !(d_isfinite(oh) && d_isfinite(ou) && d_isfinite(ov));
+#pragma unroll
+                for (int k = 0; k < CPT; ++k) {
+                    if (!out_col[k]) continue;
+                    const unsigned i = (unsigned)q * upitch + (unsigned)(cb + k);
+                    T oh = sbh[k], ou = sbu[k], ov = sbv[k];
+                    if (AVG) {
+                        oh = T(0.5) * pah[k] + T(0.5) * oh;
+                        ou = T(0.5) * pahu[k] + T(0.5) * ou;
+                        ov = T(0.5) * pahv[k] + T(0.5) * ov;
+                    }
+                    a.oh[i] = oh;
+                    a.ohu[i] = ou;
+                    a.ohv[i] = ov;
+                    bad |= !(d_isfinite(oh) && d_isfinite(ou) && d_isfinite(ov));
+                }
             }
 
             // ================= shift the windows
-            pA = pr; hA = h_r; huA = hu_r; hvA = hv_r;
-            xfA0 = xf0; xfA1 = xf1; xfA2 = xf2;
-            nfA0 = yP[0]; nfA1 = yP[1]; nfA2 = yP[2];
-            zt3 = zt2; zt2 = ztA; ztA = zt_r;
-            hr3 = hr2; hr2 = hr1; hur2 = hur1; hvr2 = hvr1;
-            mwin = (mwin << 1) | (m_r ? 1u : 0u);
-            zin4 = zin3; zin3 = zin2; zin2 = zin1; zin1 = zb_r;
-            if (!MPM) { gin4 = gin3; gin3 = gin2; gin2 = gin1; gin1 = g_r; }
-            hf4h = hf3h; hf4u = hf3u; hf4v = hf3v;
-            hf3h = hf2h; hf3u = hf2u; hf3v = hf2v;
-            e4 = e3; xe4 = xe3; fn4 = Fy;
-            zbp6 = zbp5; zbp5 = zbp4;
-            gg6 = gg5; gg5 = gg4;
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) {
+                pA[k] = pr[k]; hA[k] = h_r[k]; huA[k] = hu_r[k]; hvA[k] = hv_r[k];
+#pragma unroll
+                for (int m = 0; m < 3; ++m) { xfA[k][m] = xf[k][m]; nfA[k][m] = yP[k][m]; }
+                zt3[k] = zt2[k]; zt2[k] = ztA[k]; ztA[k] = zt_r[k];
+                hr3[k] = hr2[k]; hr2[k] = hr1[k]; hur2[k] = hur1[k]; hvr2[k] = hvr1[k];
+                mwin[k] = (mwin[k] << 1) | (m_r[k] ? 1u : 0u);
+                zin4[k] = zin3[k]; zin3[k] = zin2[k]; zin2[k] = zin1[k]; zin1[k] = zb_r[k];
+                if (!MPM) { gin4[k] = gin3[k]; gin3[k] = gin2[k]; gin2[k] = gin1[k]; gin1[k] = g_r[k]; }
+                hf4h[k] = hf3h[k]; hf4u[k] = hf3u[k]; hf4v[k] = hf3v[k];
+                hf3h[k] = hf2h[k]; hf3u[k] = hf2u[k]; hf3v[k] = hf2v[k];
+                e4[k] = e3[k]; xe4[k] = xe3[k]; fn4[k] = Fy[k];
+                zbp6[k] = zbp5[k]; zbp5[k] = zbp4[k];
+                gg6[k] = gg5[k]; gg5[k] = gg4[k];
+            }
         };
         const int steady0 = min(L0 + 5, L1), steady1 = L1;
         int r = L0;
