@@ -299,6 +299,10 @@ struct Geometry {
     int band_rows = 0, nstrips = 0, nbands = 0, grid = 0;
 };
 
+#ifndef PXB_CFL_ITEMS_PER_WARP
+#define PXB_CFL_ITEMS_PER_WARP 2
+#endif
+
 Geometry stage_geometry(int ny, int nx, int esize, int resident_warps, int want_rows) {
     Geometry g;
     const int sout = pxb_stage_strip_out(esize);
@@ -325,11 +329,15 @@ Geometry stage_geometry(int ny, int nx, int esize, int resident_warps, int want_
 Geometry cfl_geometry(int ny, int nx, int resident_warps) {
     Geometry g;
     g.nstrips = std::max(1, (nx + 30) / 31);
-    const int target_bands = std::max(1, resident_warps / g.nstrips);
-    g.band_rows = std::max(8, (ny + target_bands - 1) / target_bands);
+    // about PXB_CFL_ITEMS_PER_WARP items per resident warp, handed out by the kernel's queue
+    // so that the SMs finish together, but bands of at least 32 rows (each band re-reads one
+    // row for its first y-faces: on small grids one item per warp is faster)
+    const int target_bands = std::max(1, PXB_CFL_ITEMS_PER_WARP * resident_warps / g.nstrips);
+    g.band_rows = std::max(32, (ny + target_bands - 1) / target_bands);
     g.nbands = std::max(1, (ny + g.band_rows - 1) / g.band_rows);
     const int items = g.nstrips * g.nbands;
-    g.grid = std::max(1, (items + 7) / 8);
+    const int need = std::max(1, (items + 7) / 8), cap = std::max(1, resident_warps / 8);
+    g.grid = need >= cap / 4 ? std::min(need, cap) : need;
     return g;
 }
 

@@ -25,6 +25,8 @@ struct CflScratch {
     double t_step;               // simulation time at the start of the current step
     double t_next;               // t_step + dt: the time the next dt is added to
     unsigned int queue[2];       // stage kernel work queue: items handed out, blocks finished
+    unsigned int cfl_queue;      // CFL kernel work queue: items handed out (reset by the last block)
+    unsigned int pad2;
 };
 
 // Start of a fixed-step run at time t0 (the first CFL launch moves it into t_step).
@@ -121,7 +123,14 @@ __global__ void __launch_bounds__(256) re_cfl_kernel(const CflArgs<T> a) {
     const int nw = (gridDim.x * blockDim.x) >> 5;
     unsigned long long best = 0ull;
     const int nitems = a.nstrips * a.nbands;
-    for (int item = wid; item < nitems; item += nw) re_cfl_item<T, HAS_MASK>(a, item, best);
+    // first item by warp index, the rest from a grid-wide queue (faster warps take more)
+    int item = wid;
+    while (item < nitems) {
+        re_cfl_item<T, HAS_MASK>(a, item, best);
+        unsigned next = 0;
+        if (lane == 0) next = atomicAdd(&a.scr->cfl_queue, 1u);
+        item = nw + (int)__shfl_sync(FULL, next, 0);
+    }
     // warp max, one atomic per warp
     for (int o = 16; o > 0; o >>= 1) {
         const unsigned long long other = __shfl_xor_sync(FULL, best, o);
@@ -156,6 +165,7 @@ __global__ void __launch_bounds__(256) re_cfl_kernel(const CflArgs<T> a) {
         if (!d_isfinite(dt)) a.scr->err |= 2;
         a.scr->maxbits = 0ull;
         a.scr->done = 0u;
+        a.scr->cfl_queue = 0u;  // every warp has left its item loop
         __threadfence();
     }
 }
