@@ -194,11 +194,23 @@ __device__ __forceinline__ void roe_exner_face(const HCell<T>& I, const HCell<T>
         //   upwP = (A1 + A3, A1 l1 + A3 l3, (A1 + A3) vt + [ut > 0] w2 ct)
         //   upwM = the same with T_k - A_k and [ut <= 0].
         // (b1, w2c, e1, e3 are rounded products, so each sum below has one product to fuse)
+        // When no face of the warp needs the entropy fix (the vote above; lambda_E = 0) the
+        // e_k terms are dropped for the whole warp; they add only zeros then (the sign of a
+        // zero flux component may differ, which no update can see).
         const float w1 = __fmaf_rn(l1, a1, -b1), w2c = mul_rn(ut * a2, ct), w3 = __fmaf_rn(l3, a3, -b3);
-        const float e1 = mul_rn(lE1, a1), e3 = mul_rn(lE3, a3);
-        const float A1 = (l1 > 0.f ? w1 : 0.f) + (lE1 > 0.f ? e1 : 0.f);
-        const float A3 = (l3 > 0.f ? w3 : 0.f) + (lE3 > 0.f ? e3 : 0.f);
-        const float B1 = (w1 + e1) - A1, B3 = (w3 + e3) - A3;
+        float A1, A3, B1, B3;
+        if (need) {
+            const float e1 = mul_rn(lE1, a1), e3 = mul_rn(lE3, a3);
+            A1 = (l1 > 0.f ? w1 : 0.f) + (lE1 > 0.f ? e1 : 0.f);
+            A3 = (l3 > 0.f ? w3 : 0.f) + (lE3 > 0.f ? e3 : 0.f);
+            B1 = (w1 + e1) - A1;
+            B3 = (w3 + e3) - A3;
+        } else {
+            A1 = l1 > 0.f ? w1 : 0.f;
+            A3 = l3 > 0.f ? w3 : 0.f;
+            B1 = w1 - A1;  // as (w1 + e1) - A1, NaN included
+            B3 = w3 - A3;
+        }
         const bool s2 = ut > 0.f;
         p0 = A1 + A3;
         p1 = sum2(A1, l1, A3, l3);
