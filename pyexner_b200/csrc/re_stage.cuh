@@ -525,7 +525,26 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
 
             // ================= C: momentum corrections of row r-2
             T hf2h[CPT], hf2u[CPT], hf2v[CPT];
-            {
+            // Where every cell of the warp is wet and its north / south neighbours are not
+            // dry (no nodata mask), no correction applies: a warp vote skips the tests and
+            // their shuffles.  Exact: NaN depths fail the vote, as they fail `active`.
+            bool allwet = false;
+            if constexpr (!HAS_MASK) {
+                bool dry = false;
+#pragma unroll
+                for (int k = 0; k < CPT; ++k)
+                    dry = dry || (colok[k] && (!(hr2[k] > DRY) || (hr3[k] < DRY) || (hr1[k] < DRY)));
+                allwet = !__any_sync(FULL, dry);
+            }
+            if (allwet) {
+#pragma unroll
+                for (int k = 0; k < CPT; ++k) {
+                    const bool ok = S || (r - 2 >= L0 && r - 2 < L1);
+                    hf2h[k] = ok ? hr2[k] : T(0);
+                    hf2u[k] = ok ? hur2[k] : T(0);
+                    hf2v[k] = ok ? hvr2[k] : T(0);
+                }
+            } else {
                 const int q2 = r - 2;
                 T hE[CPT], hW[CPT], zE[CPT], zW[CPT];
                 bool m2[CPT], mE[CPT], mW[CPT];
