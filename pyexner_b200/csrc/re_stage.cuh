@@ -690,15 +690,10 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
                     const T Gq = MPM ? mpm_grass(hbh[k], hbu[k], hbv[k], mq[k], a.sed) : const_grass(hbh[k], gb1[k], mq[k]);
                     e3[k] = make_ecell(hbh[k], hbu[k], hbv[k], zb1[k], Gq);
                 }
-                ECell<T> ee[CPT];
-                bool mqe[CPT];
-#pragma unroll
-                for (int k = 0; k + 1 < CPT; ++k) { ee[k] = e3[k + 1]; mqe[k] = mq[k + 1]; }
-                ee[CPT - 1] = shfl_down_ecell(e3[0]);
-                mqe[CPT - 1] = HAS_MASK ? (__shfl_down_sync(FULL, (int)mq[0], 1) != 0) : false;
-                // Below the Shields threshold G is 0 and every Exner flux of the face is 0
-                // (q = G |u|^2 u): in float32 a warp whose rows q and q-1 carry no G skips the
-                // face arithmetic (a NaN G is not 0, so it still propagates).
+                // Below the Shields threshold G is 0 and every Exner flux is 0 (q = G |u|^2 u):
+                // in float32 a warp whose rows q and q-1 carry no G skips the Exner faces,
+                // their shuffles and activity tests; xe3 and Fy keep their +0 (exact, and a
+                // NaN G is not 0, so it still propagates).
                 bool sed = true;
                 if constexpr (is_f32<T>()) {
                     bool anyG = false;
@@ -706,28 +701,36 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
                     for (int k = 0; k < CPT; ++k) anyG = anyG || !(e3[k].G == T(0)) || !(e4[k].G == T(0));
                     sed = __any_sync(FULL, anyG);
                 }
-                T F[CPT];
-                bool xact[CPT];
+                if (sed) {
+                    ECell<T> ee[CPT];
+                    bool mqe[CPT];
 #pragma unroll
-                for (int k = 0; k < CPT; ++k) {
-                    xact[k] = rowD && has_e[k] && exner_active(e3[k], ee[k], mq[k], mqe[k]);
-                    const T Fx = sed ? exner_face<T, false>(e3[k], ee[k]) : T(0);
-                    F[k] = xact[k] ? Fx : T(0);
-                }
-                T Fw[CPT];
-                bool wact[CPT];
+                    for (int k = 0; k + 1 < CPT; ++k) { ee[k] = e3[k + 1]; mqe[k] = mq[k + 1]; }
+                    ee[CPT - 1] = shfl_down_ecell(e3[0]);
+                    mqe[CPT - 1] = HAS_MASK ? (__shfl_down_sync(FULL, (int)mq[0], 1) != 0) : false;
+                    T F[CPT];
+                    bool xact[CPT];
 #pragma unroll
-                for (int k = 1; k < CPT; ++k) { Fw[k] = F[k - 1]; wact[k] = xact[k - 1]; }
-                Fw[0] = __shfl_up_sync(FULL, F[CPT - 1], 1);
-                wact[0] = (__shfl_up_sync(FULL, (int)xact[CPT - 1], 1) != 0) && lane > 0;
+                    for (int k = 0; k < CPT; ++k) {
+                        xact[k] = rowD && has_e[k] && exner_active(e3[k], ee[k], mq[k], mqe[k]);
+                        const T Fx = exner_face<T, false>(e3[k], ee[k]);
+                        F[k] = xact[k] ? Fx : T(0);
+                    }
+                    T Fw[CPT];
+                    bool wact[CPT];
 #pragma unroll
-                for (int k = 0; k < CPT; ++k) {
-                    // roe_exner.py:710-711: -F of the west face first, then +F of the east face
-                    if (wact[k]) xe3[k] = xe3[k] + (-Fw[k]);
-                    if (xact[k]) xe3[k] = xe3[k] + F[k];
-                    const bool yex = rowD && (S || q - 1 >= L0) && colok[k] && exner_active(e4[k], e3[k], mq1[k], mq[k]);
-                    const T Fyv = sed ? exner_face<T, true>(e4[k], e3[k]) : T(0);
-                    Fy[k] = yex ? Fyv : T(0);
+                    for (int k = 1; k < CPT; ++k) { Fw[k] = F[k - 1]; wact[k] = xact[k - 1]; }
+                    Fw[0] = __shfl_up_sync(FULL, F[CPT - 1], 1);
+                    wact[0] = (__shfl_up_sync(FULL, (int)xact[CPT - 1], 1) != 0) && lane > 0;
+#pragma unroll
+                    for (int k = 0; k < CPT; ++k) {
+                        // roe_exner.py:710-711: -F of the west face first, then +F of the east face
+                        if (wact[k]) xe3[k] = xe3[k] + (-Fw[k]);
+                        if (xact[k]) xe3[k] = xe3[k] + F[k];
+                        const bool yex = rowD && (S || q - 1 >= L0) && colok[k] && exner_active(e4[k], e3[k], mq1[k], mq[k]);
+                        const T Fyv = exner_face<T, true>(e4[k], e3[k]);
+                        Fy[k] = yex ? Fyv : T(0);
+                    }
                 }
             }
 
