@@ -21,6 +21,8 @@ Reported:
              the same generator, about 10 s of CPU work;
   plain_roe  configuration 1: the plain Roe dam-break (256^2, float64, SSPRK2, 200 steps)
              and the NumPy oracle on the host for 10 steps of it;
+  transport_case  the same case started at u = 1 m/s (Shields number about 0.15, bedload
+             in every cell, so the stage kernel's sediment-free fast path never fires);
   ensemble   the ragged ensemble workload (64 Roe-Exner dam breaks, sides U{128..1024},
              own beds, step heights and dts; float32; 1000 SSPRK2 steps): autotuned band
              height, cell-updates/s over all members (state ~1.1 GB, larger than L2).
@@ -169,12 +171,12 @@ def replica_throughput(world, cells, steps, sec):
     return world * cells * steps / sec
 
 
-def build_case(n, dtype, device):
+def build_case(n, dtype, device, u0=0.1):
     import torch
 
     from pyexner_b200 import RoeExnerState, cases, create_solver_bundle
 
-    c = cases.gaussian_bed(n, device=device)
+    c = cases.gaussian_bed(n, device=device, u0=u0)
     st = RoeExnerState.from_numpy(c["arrs"], c["seds"], dtype)
     bundle = create_solver_bundle("Roe Exner")
     cfg = bundle.config(st, None, c["boundaries"], c["dx"], c["params"])
@@ -479,6 +481,8 @@ def main():
     ap.add_argument("--accuracy-steps", type=int, default=2000)
     ap.add_argument("--n-big", type=int, default=8192, help="side of the bandwidth case (0 to skip)")
     ap.add_argument("--big-steps", type=int, default=20)
+    ap.add_argument("--transport-u", type=float, default=1.0,
+                    help="initial velocity of the bedload-everywhere variant of the case (0 to skip)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ensemble-members", type=int, default=64, help="ragged ensemble size (0 to skip)")
     ap.add_argument("--ensemble-steps", type=int, default=1000)
@@ -556,6 +560,19 @@ def main():
     sec64, _ = timed_device_loop(st64, mask64, cfg64, max(3, args.steps // 2), args.warmup, flush)
     value64 = ncell * max(3, args.steps // 2) / sec64
     del st64
+    # ---- the same case with bedload everywhere (u0 = 1 m/s): the stage kernel's
+    # sediment-free fast path never fires there
+    transport = None
+    if args.transport_u > 0:
+        ct, bt, cfgt, maskt, stt = build_case(n, torch.float32, "cuda", u0=args.transport_u)
+        sect, bscr = timed_device_loop(stt, maskt, cfgt, args.steps, args.warmup, flush)
+        ktt = kernel_breakdown(stt, bscr, maskt, cfgt, max(3, args.steps // 2), flush)
+        gpos = float((stt.G[1:-1, 1:-1] > 0).float().mean().item())
+        transport = {"workload": f"roe_exner_gaussian_bed_{n}x{n}_mpm_ssprk2_f32_u{args.transport_u:g}",
+                     "value": ncell * args.steps / sect, "unit": UNIT, "steps": args.steps,
+                     "cells_with_bedload": gpos, "ms": {k: 1e3 * v for k, v in ktt.items()}}
+        del stt, bscr
+        torch.cuda.empty_cache()
     # ---- end to end through the public API with host buffers
     e2e_sec, h2d, d2h = e2e_run(n, torch.float32, args.steps, args.warmup)
     e2e_val = ncell * args.steps / e2e_sec
@@ -584,6 +601,7 @@ def main():
                      "ms": {k: 1e3 * v for k, v in kt.items()}},
         "fp64": {"value": value64, "unit": UNIT, "fp32_over_fp64": value / world / value64},
         "bandwidth_case": big,
+        "transport_case": transport,
         "ensemble": ens,
         "plain_roe": roe,
         "accuracy": acc,

@@ -47,19 +47,21 @@ def dambreak_roe(n=256):
     return dict(arrs=arrs, dx=dx, params=params, boundaries=BoundaryManager(params, X, Y), X=X, Y=Y)
 
 
-def gaussian_bed_fields(n, dx=0.01, seed_bed=1, seed_noise=2, device=None):
+def gaussian_bed_fields(n, dx=0.01, seed_bed=1, seed_noise=2, device=None, u0=0.1):
     """Planes of the Gaussian-bed case as float64 numpy arrays (ring included).
 
     With ``device`` set (e.g. "cuda") the bed sum is evaluated with torch on that device,
     which is what makes the 8192^2 case quick to build; the numbers are the same
-    float64 expression either way."""
+    float64 expression either way.  ``u0`` is the initial velocity (hu = u0 h): the
+    default 0.1 m/s keeps the Shields number near 1.5e-3, far below the threshold 0.047
+    (no bedload at the start); 1 m/s gives about 0.15, bedload everywhere."""
     zt = gaussian_bed_total(n, n, dx, seed_bed, device)
     z = np.full(zt.shape, zt.min() - 0.05)
     zb = zt - z
     rn = np.random.default_rng(seed_noise)
     noise = rn.uniform(-1.0, 1.0, zt.shape)
     h = np.maximum(0.0, (0.3 - zt) * (1.0 + 0.02 * noise))
-    return dict(h=h, hu=0.1 * h, hv=np.zeros_like(h), z=z, z_b=zb, n=np.zeros_like(h), G=np.zeros_like(h))
+    return dict(h=h, hu=u0 * h, hv=np.zeros_like(h), z=z, z_b=zb, n=np.zeros_like(h), G=np.zeros_like(h))
 
 
 def gaussian_bed_total(ny_phys, nx_phys, dx=0.01, seed_bed=1, device=None):
@@ -96,9 +98,9 @@ def gaussian_bed_total(ny_phys, nx_phys, dx=0.01, seed_bed=1, device=None):
     return zt
 
 
-def gaussian_bed(n, dx=0.01, seed_bed=1, seed_noise=2, device=None):
+def gaussian_bed(n, dx=0.01, seed_bed=1, seed_noise=2, device=None, u0=0.1):
     ny = nx = n + 2
-    arrs = gaussian_bed_fields(n, dx, seed_bed, seed_noise, device)
+    arrs = gaussian_bed_fields(n, dx, seed_bed, seed_noise, device, u0)
     erosion = dict(grass_factor="MPM", bulk_porosity=0.42, sediments=SED_ONE)
     bspec = ring_boundaries(ny, nx, ["Transmissive", "TransmissiveBed"], ["Transmissive", "TransmissiveBed"],
                             ["Reflective"], ["Reflective"])
