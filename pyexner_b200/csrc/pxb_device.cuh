@@ -505,7 +505,7 @@ __device__ __forceinline__ T face_speed(const CCell<T>& I, const CCell<T>& J) {
     const T gt = T(0.5) * (I.G + J.G);
     T ut, ct, at;
     if constexpr (is_f32<T>()) {
-        ut = sum2(uhi, I.sq, uhj, J.sq) * f_rcp(den);
+        ut = mul_rn(sum2(uhi, I.sq, uhj, J.sq), f_rcp(den));  // rounded: u~ -+ c~ as in face_speed_nog
         ct = f_sqrt(9.81f * ht);
         const float s4 = __fmaf_rn(vhi, vhj, __fmaf_rn(uhj, uhj, fsum2(uhi, uhi, uhi, uhj)));
         at = gt * s4 * (I.rs * J.rs);
@@ -520,6 +520,25 @@ __device__ __forceinline__ T face_speed(const CCell<T>& I, const CCell<T>& J) {
     const T roe = nan_max(fabs(lmin), fabs(lmax));
     const T swe = nan_max(fabs(l1), fabs(l3));
     return roe < T(VEL_TOL) ? swe : roe;
+}
+
+// face_speed of a face whose two cells carry no G (G = 0, so a~ = 0 and the cubic's
+// extreme roots are u~ -+ c~): the same value, without a~ and the cubic branch.
+template <class T, bool YF>
+__device__ __forceinline__ T face_speed_nog(const CCell<T>& I, const CCell<T>& J) {
+    const T uhi = YF ? -I.v : I.u;
+    const T uhj = YF ? -J.v : J.u;
+    const T den = I.sq + J.sq;
+    const T ht = T(0.5) * (I.h + J.h);
+    T ut, ct;
+    if constexpr (is_f32<T>()) {
+        ut = mul_rn(sum2(uhi, I.sq, uhj, J.sq), f_rcp(den));
+        ct = f_sqrt(9.81f * ht);
+    } else {
+        ut = (uhi * I.sq + uhj * J.sq) / den;
+        ct = d_sqrt(T(G_ACC) * ht);
+    }
+    return nan_max(fabs(ut - ct), fabs(ut + ct));
 }
 
 // Order-preserving map of a non-negative (or NaN) float to unsigned bits for atomicMax.

@@ -90,6 +90,10 @@ __device__ __forceinline__ void re_cfl_item(const CflArgs<T>& a, const int item,
             const bool m = nm;
             fetch(r + 1);
             const CCell<T> cur = make_ccell(h, hu, hv, g);
+            // float32: rows r-1 and r of the warp without G (below the Shields threshold)
+            // take face_speed_nog, the same value without the cubic (a NaN G is not 0)
+            bool nog = false;
+            if constexpr (is_f32<T>()) nog = !__any_sync(FULL, !(g == T(0)) || !(prev.G == T(0)));
             if (r < R1) {  // x-face (c | c+1) of row r
                 CCell<T> e;
                 e.h = __shfl_down_sync(FULL, cur.h, 1);
@@ -101,12 +105,14 @@ __device__ __forceinline__ void re_cfl_item(const CflArgs<T>& a, const int item,
                 const T he = __shfl_down_sync(FULL, h, 1);
                 const bool me = HAS_MASK ? (__shfl_down_sync(FULL, (int)m, 1) != 0) : false;
                 if (has_e && ((h > DRY) || (he > DRY)) && !(m || me)) {
-                    const unsigned long long b = speed_bits(face_speed<T, false>(cur, e));
+                    const unsigned long long b =
+                        speed_bits(nog ? face_speed_nog<T, false>(cur, e) : face_speed<T, false>(cur, e));
                     best = b > best ? b : best;
                 }
             }
             if (r > R0 && colok && ((hprev > DRY) || (h > DRY)) && !(mprev || m)) {  // y-face (r-1 | r)
-                const unsigned long long b = speed_bits(face_speed<T, true>(prev, cur));
+                const unsigned long long b =
+                    speed_bits(nog ? face_speed_nog<T, true>(prev, cur) : face_speed<T, true>(prev, cur));
                 best = b > best ? b : best;
             }
             prev = cur;
