@@ -13,6 +13,7 @@
 // by one column) and marches down a band of rows; y-faces (r | r+1) belong to row r's band.
 #pragma once
 #include "pxb_device.cuh"
+#include "re_stage.cuh"  // cp.async helpers
 
 namespace pxb {
 
@@ -68,25 +69,61 @@ __device__ __forceinline__ void re_cfl_item(const CflArgs<T>& a, const int item,
         T hprev = 0;
         bool mprev = false;
         const int rend = min(ny, R1 + 1);
-        // row r+1 is loaded while row r is evaluated
+        // float32: rows arrive by cp.async in this warp's shared slots two rows ahead (the
+        // kernel is memory-latency bound with one row of register prefetch); float64 keeps
+        // the register prefetch of row r+1.  The nodata byte is a register prefetch.
+        constexpr bool ASYNC = is_f32<T>();
+        __shared__ T cbuf[8][ASYNC ? 3 : 1][4][32];
+        T(*cb)[4][32] = cbuf[(threadIdx.x >> 5) & 7];
         T nh = 1, nhu = 0, nhv = 0, ng = 0;
         bool nm = false;
-        auto fetch = [&](int rr) {
-            nh = 1;
-            nhu = nhv = ng = 0;
-            nm = false;
+        auto issue = [&](int rr) __attribute__((always_inline)) {  // float32: row rr into slot rr % 3
+            T* d = &cb[rr % 3][0][lane];
             if (colok && rr < rend) {
                 const long long i = (long long)rr * a.pitch + c;
-                nh = __ldg(a.h + i);
-                nhu = __ldg(a.hu + i);
-                nhv = __ldg(a.hv + i);
-                ng = __ldg(a.G + i);
+                cp_async_elem(d, a.h + i);
+                cp_async_elem(d + 32, a.hu + i);
+                cp_async_elem(d + 64, a.hv + i);
+                cp_async_elem(d + 96, a.G + i);
+            } else {
+                d[0] = T(1);
+                d[32] = d[64] = d[96] = T(0);
+            }
+            cp_async_commit();
+        };
+        auto fetch = [&](int rr) __attribute__((always_inline)) {
+            nm = false;
+            if constexpr (!ASYNC) {
+                nh = 1;
+                nhu = nhv = ng = 0;
+            }
+            if (colok && rr < rend) {
+                const long long i = (long long)rr * a.pitch + c;
+                if constexpr (!ASYNC) {
+                    nh = __ldg(a.h + i);
+                    nhu = __ldg(a.hu + i);
+                    nhv = __ldg(a.hv + i);
+                    ng = __ldg(a.G + i);
+                }
                 if (HAS_MASK) nm = __ldg(a.nodata + i) != 0;
             }
         };
+        if constexpr (ASYNC) {
+            issue(R0);
+            issue(R0 + 1);
+        }
         fetch(R0);
         for (int r = R0; r < rend; ++r) {
-            const T h = nh, hu = nhu, hv = nhv, g = ng;
+            T h = nh, hu = nhu, hv = nhv, g = ng;
+            if constexpr (ASYNC) {
+                cp_async_wait<1>();  // row r landed (row r+1 may be in flight); each lane reads its own slots
+                const T* sr = &cb[r % 3][0][lane];
+                h = sr[0];
+                hu = sr[32];
+                hv = sr[64];
+                g = sr[96];
+                issue(r + 2);
+            }
             const bool m = nm;
             fetch(r + 1);
             const CCell<T> cur = make_ccell(h, hu, hv, g);
@@ -119,6 +156,7 @@ __device__ __forceinline__ void re_cfl_item(const CflArgs<T>& a, const int item,
             hprev = h;
             mprev = m;
         }
+        if constexpr (ASYNC) cp_async_wait<0>();  // the slots are reused by the next item
     }
 }
 
