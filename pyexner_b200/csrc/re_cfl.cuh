@@ -127,10 +127,9 @@ __device__ __forceinline__ void re_cfl_item(const CflArgs<T>& a, const int item,
             const bool m = nm;
             fetch(r + 1);
             const CCell<T> cur = make_ccell(h, hu, hv, g);
-            // float32: rows r-1 and r of the warp without G (below the Shields threshold)
-            // take face_speed_nog, the same value without the cubic (a NaN G is not 0)
-            bool nog = false;
-            if constexpr (is_f32<T>()) nog = !__any_sync(FULL, !(g == T(0)) || !(prev.G == T(0)));
+            // rows r-1 and r of the warp without G (below the Shields threshold) take
+            // face_speed_nog, the same value without a~ and the cubic (a NaN G is not 0)
+            const bool nog = !__any_sync(FULL, !(g == T(0)) || !(prev.G == T(0)));
             if (r < R1) {  // x-face (c | c+1) of row r
                 CCell<T> e;
                 e.h = __shfl_down_sync(FULL, cur.h, 1);

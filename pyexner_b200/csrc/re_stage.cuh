@@ -691,17 +691,14 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
                     e3[k] = make_ecell(hbh[k], hbu[k], hbv[k], zb1[k], Gq);
                 }
                 // Below the Shields threshold G is 0 and every Exner flux is 0 (q = G |u|^2 u):
-                // in float32 a warp whose rows q and q-1 carry no G skips the Exner faces,
-                // their shuffles and activity tests; xe3 and Fy keep their +0 (exact, and a
-                // NaN G is not 0, so it still propagates).
-                bool sed = true;
-                if constexpr (is_f32<T>()) {
-                    bool anyG = false;
+                // a warp whose rows q and q-1 carry no G skips the Exner faces, their shuffles
+                // and activity tests; xe3 and Fy keep their +0.  Exact in both precisions: the
+                // skipped fluxes are +-0, which leave z_b unchanged bit for bit, and a NaN G
+                // (NaN depth or velocity in the MPM factor) is not 0, so it still propagates.
+                bool anyG = false;
 #pragma unroll
-                    for (int k = 0; k < CPT; ++k) anyG = anyG || !(e3[k].G == T(0)) || !(e4[k].G == T(0));
-                    sed = __any_sync(FULL, anyG);
-                }
-                if (sed) {
+                for (int k = 0; k < CPT; ++k) anyG = anyG || !(e3[k].G == T(0)) || !(e4[k].G == T(0));
+                if (__any_sync(FULL, anyG)) {
                     ECell<T> ee[CPT];
                     bool mqe[CPT];
 #pragma unroll
