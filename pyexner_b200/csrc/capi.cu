@@ -330,10 +330,14 @@ Geometry cfl_geometry(int ny, int nx, int resident_warps) {
     Geometry g;
     g.nstrips = std::max(1, (nx + 30) / 31);
     // about PXB_CFL_ITEMS_PER_WARP items per resident warp, handed out by the kernel's queue
-    // so that the SMs finish together, but bands of at least 32 rows (each band re-reads one
-    // row for its first y-faces: on small grids one item per warp is faster)
+    // so that the SMs finish together; where that would make bands shorter than 32 rows
+    // (each band re-reads one row for its first y-faces) one item per warp is faster
     const int target_bands = std::max(1, PXB_CFL_ITEMS_PER_WARP * resident_warps / g.nstrips);
-    g.band_rows = std::max(32, (ny + target_bands - 1) / target_bands);
+    g.band_rows = (ny + target_bands - 1) / target_bands;
+    if (g.band_rows < 32) {
+        const int one = std::max(1, resident_warps / g.nstrips);
+        g.band_rows = std::max(8, (ny + one - 1) / one);
+    }
     g.nbands = std::max(1, (ny + g.band_rows - 1) / g.band_rows);
     const int items = g.nstrips * g.nbands;
     const int need = std::max(1, (items + 7) / 8), cap = std::max(1, resident_warps / 8);

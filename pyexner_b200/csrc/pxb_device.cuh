@@ -297,23 +297,29 @@ template <class T, bool YF>
 __device__ __forceinline__ T exner_face(const ECell<T>& I, const ECell<T>& J) {
     const T uhi = YF ? -I.v : I.u;
     const T uhj = YF ? -J.v : J.u;
-    const T qi = mul_rn(I.G * I.um, uhi);
-    const T qj = mul_rn(J.G * J.um, uhj);
     const T gt = T(0.5) * (I.G + J.G);
     const T dz = J.zbe - I.zbe;
-    const T qbi = qi + (gt - I.G) * I.um * uhi;
-    const T qbj = qj + (gt - J.G) * J.um * uhj;
     // lambda_4 = dq/dz, or the Roe-averaged normal velocity when |dz| <= SED_TOL; only
     // its sign is used.  Products are rounded separately (no FMA) so that exact
     // cancellations stay exact, as in the reference's arithmetic.
     const bool big = fabs(dz) > T(SED_TOL);
-    bool up;
     if constexpr (is_f32<T>()) {
-        const float dq = mul_rn(mul_rn(gt, J.um), uhj) - mul_rn(mul_rn(gt, I.um), uhi);
+        // q_b + corrector = G q + (G~ - G) |u|^2 u = G~ |u|^2 u: the float build takes the
+        // two products of dq as the upwind fluxes (the float64 build keeps the reference's
+        // two-term form)
+        const float pi = mul_rn(mul_rn(gt, I.um), uhi), pj = mul_rn(mul_rn(gt, J.um), uhj);
+        const float dq = pj - pi;
         const bool up_big = (dq == 0.f) || (dq == dq && ((dq > 0.f) == (dz > 0.f)));
         const float num = mul_rn(uhi, I.sq) + mul_rn(uhj, J.sq);  // sign of ut (denominator > 0)
-        up = big ? up_big : (num >= 0.f);
-    } else {
+        const bool up = big ? up_big : (num >= 0.f);
+        return up ? pi : pj;
+    }
+    const T qi = mul_rn(I.G * I.um, uhi);
+    const T qj = mul_rn(J.G * J.um, uhj);
+    const T qbi = qi + (gt - I.G) * I.um * uhi;
+    const T qbj = qj + (gt - J.G) * J.um * uhj;
+    bool up;
+    {
         const T ut = (uhi * I.sq + uhj * J.sq) / (I.sq + J.sq);
         const T dq = gt * J.um * uhj - gt * I.um * uhi;
         const T lam4 = big ? dq / dz : ut;
