@@ -365,13 +365,26 @@ __device__ __forceinline__ T mpm_grass(T h, T hu, T hv, bool nodata, const SedTa
     if constexpr (is_f32<T>()) {
         // G = sum_k frac n_p^3 sqrt(g)/((s-1) sqrt h) * 8 sqrt(dth)/(th^1.5 + 1e-5) * dth
         const float hc = clamp_lo(h, float(DRY_TOL));
-        // one Newton step each: the threshold (theta - theta_c)^1.5 amplifies errors in theta
         float rs = f_rsqrt(hc);
+        float rcb = f_ex2(-0.33333333333f * f_lg2(hc));  // h^(-1/3)
+        {
+            // Below the Shields threshold in every lane and class G is 0.  The unrefined
+            // theta (relative error under 1e-5) decides it with a 1e-4 margin, so such warps
+            // return before the refinement; the full evaluation gives the same 0 there (and
+            // 0 for a NaN depth or velocity too).
+            const float r0 = rs * rs;
+            const float u0 = hu * r0, v0 = hv * r0;
+            const float q0 = fsum2(u0, u0, v0, v0) * rcb;
+            bool above = false;
+#pragma unroll 1
+            for (int k = 0; k < S.n; ++k) above = above || (S.k_theta[k] * q0 > 0.9999f * S.s[k].thc);
+            if (!__any_sync(FULL, above)) return 0.f;
+        }
+        // one Newton step each: the threshold (theta - theta_c)^1.5 amplifies errors in theta
         rs = rs * (1.5f - 0.5f * hc * rs * rs);
         const float r = rs * rs;
         const float u = hu * r, v = hv * r;
         const float vel2 = fsum2(u, u, v, v);
-        float rcb = f_ex2(-0.33333333333f * f_lg2(hc));  // h^(-1/3)
         rcb = rcb * (4.f - hc * rcb * rcb * rcb) * (1.f / 3.f);
         float G = 0.f;
 #pragma unroll 1

@@ -442,18 +442,17 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
             // skipped for the whole warp (r is warp-uniform); their results would be masked.
             if (S || rowA) {
                 HCell<T> pe[CPT];
-                T he[CPT];
                 bool me[CPT];
 #pragma unroll
-                for (int k = 0; k + 1 < CPT; ++k) { pe[k] = pr[k + 1]; he[k] = h_r[k + 1]; me[k] = m_r[k + 1]; }
+                for (int k = 0; k + 1 < CPT; ++k) { pe[k] = pr[k + 1]; me[k] = m_r[k + 1]; }
                 pe[CPT - 1] = shfl_down_hcell(pr[0]);
-                he[CPT - 1] = __shfl_down_sync(FULL, h_r[0], 1);
                 me[CPT - 1] = HAS_MASK ? (__shfl_down_sync(FULL, (int)m_r[0], 1) != 0) : false;
                 T P[CPT][3], M[CPT][3];
                 bool xact[CPT];
 #pragma unroll
                 for (int k = 0; k < CPT; ++k) {
-                    xact[k] = rowA && has_e[k] && ((h_r[k] > DRY) || (he[k] > DRY)) && !(m_r[k] || me[k]);
+                    // pr.h = max(h, DRY_TOL) > DRY_TOL exactly when h > DRY_TOL (false for NaN)
+                    xact[k] = rowA && has_e[k] && ((pr[k].h > DRY) || (pe[k].h > DRY)) && !(m_r[k] || me[k]);
                     roe_exner_face<T, false>(pr[k], pe[k], dx, P[k], M[k]);
 #pragma unroll
                     for (int m = 0; m < 3; ++m) {
@@ -462,25 +461,24 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
                     }
                 }
                 // upwP of the west face of column k: own column k-1, or the west lane's last
+                // (lane 0 has no west face in the warp).  P and M are zero on inactive faces,
+                // and the sums start at +0, so adding them unconditionally gives the same bits
+                // as adding only the active ones.
                 T wP[CPT][3];
-                bool wact[CPT];
 #pragma unroll
-                for (int k = 1; k < CPT; ++k) {
-                    wact[k] = xact[k - 1];
+                for (int k = 1; k < CPT; ++k)
 #pragma unroll
                     for (int m = 0; m < 3; ++m) wP[k][m] = P[k - 1][m];
-                }
 #pragma unroll
-                for (int m = 0; m < 3; ++m) wP[0][m] = __shfl_up_sync(FULL, P[CPT - 1][m], 1);
-                wact[0] = (__shfl_up_sync(FULL, (int)xact[CPT - 1], 1) != 0) && lane > 0;
+                for (int m = 0; m < 3; ++m) {
+                    const T w = __shfl_up_sync(FULL, P[CPT - 1][m], 1);
+                    wP[0][m] = lane > 0 ? w : T(0);
+                }
                 // scatter order of roe_exner.py:599-600: east upwM first, then west upwP
 #pragma unroll
                 for (int k = 0; k < CPT; ++k) {
 #pragma unroll
-                    for (int m = 0; m < 3; ++m) {
-                        if (xact[k]) xf[k][m] = xf[k][m] + M[k][m];
-                        if (wact[k]) xf[k][m] = xf[k][m] + wP[k][m];
-                    }
+                    for (int m = 0; m < 3; ++m) xf[k][m] = (xf[k][m] + M[k][m]) + wP[k][m];
                 }
             }
             T yP[CPT][3], yM[CPT][3];
