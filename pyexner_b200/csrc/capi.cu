@@ -302,6 +302,9 @@ struct Geometry {
 #ifndef PXB_CFL_ITEMS_PER_WARP
 #define PXB_CFL_ITEMS_PER_WARP 2
 #endif
+#ifndef PXB_CFL_MIN_ROWS
+#define PXB_CFL_MIN_ROWS 32
+#endif
 
 Geometry stage_geometry(int ny, int nx, int esize, int resident_warps, int want_rows) {
     Geometry g;
@@ -330,11 +333,12 @@ Geometry cfl_geometry(int ny, int nx, int resident_warps) {
     Geometry g;
     g.nstrips = std::max(1, (nx + 30) / 31);
     // about PXB_CFL_ITEMS_PER_WARP items per resident warp, handed out by the kernel's queue
-    // so that the SMs finish together; where that would make bands shorter than 32 rows
-    // (each band re-reads one row for its first y-faces) one item per warp is faster
+    // so that the SMs finish together; where that would make bands shorter than
+    // PXB_CFL_MIN_ROWS rows (each band re-reads one row for its first y-faces) one item per
+    // warp is faster
     const int target_bands = std::max(1, PXB_CFL_ITEMS_PER_WARP * resident_warps / g.nstrips);
     g.band_rows = (ny + target_bands - 1) / target_bands;
-    if (g.band_rows < 32) {
+    if (g.band_rows < PXB_CFL_MIN_ROWS) {
         const int one = std::max(1, resident_warps / g.nstrips);
         g.band_rows = std::max(8, (ny + one - 1) / one);
     }
