@@ -82,6 +82,28 @@ def test_members_match_single_runs(dtype, scheme, steps):
             assert np.array_equal(got[f], st_ref[f]), (k, f)
 
 
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "f32"])
+def test_large_members_take_items_from_the_work_queue(dtype):
+    """Members large enough, with 8-row bands, that the ensemble's work items outnumber the
+    resident warps several times over: a warp's first item is its index, the rest come
+    from the ensemble kernel's queue, and members change under a warp between items.  The
+    members must still give the bits of their single runs (which use the default bands)."""
+    from pyexner_b200.ensemble import Ensemble
+
+    members, erosion = make_members([(700, 650), (512, 700), (640, 600)], dtype, seed=9)
+    ref = single_runs(members, "SSPRK2", 3)
+    ens = Ensemble(members, erosion, band_rows=8)
+    ens.init()
+    dts = ens.run(3, "SSPRK2", 0.5).cpu().numpy()
+    ens.check()
+    for k, mb in enumerate(members):
+        got = mb["state"].to_numpy()
+        st_ref, dts_ref = ref[k]
+        assert np.array_equal(dts[:, k], dts_ref), k
+        for f in FIELDS:
+            assert np.array_equal(got[f], st_ref[f]), (k, f)
+
+
 def test_autotune_keeps_the_states_and_the_results():
     from pyexner_b200.ensemble import Ensemble
 
