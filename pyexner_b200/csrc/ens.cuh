@@ -1,7 +1,7 @@
 // Ragged ensembles: many independent Roe-Exner grids (each with its own size, state,
 // boundary recipes and dt) advanced together, one launch per phase for all members.
 //
-// The work items of every member (32-column strips x row bands, as in the single-grid
+// The work items of every member (warp strips x row bands, as in the single-grid
 // kernels) are numbered consecutively, member after member; a persistent grid covers the
 // global item range (first item by warp index, the rest from a work queue).  A warp finds
 // the member of its item by binary search in the item offsets and keeps that member's

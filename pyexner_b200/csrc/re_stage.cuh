@@ -6,8 +6,8 @@
 // handlers, and for the second SSPRK2 stage the 0.5/0.5 combination (SSPRK2.py:40).
 //
 // Layout of the work: a warp owns a strip of 32 x CPT columns (3 halo | owned | 3 halo;
-// CPT = 2 consecutive columns per lane in float32, 1 in float64) and marches down a band
-// of rows.  Each iteration consumes one new row, copied into the
+// CPT consecutive columns per lane, one by default, two as a float32 build knob) and
+// marches down a band of rows.  Each iteration consumes one new row, copied into the
 // warp's shared buffer by cp.async during the previous iteration (together with the
 // partner-state values the averaging stage stores in this one), and advances a software
 // pipeline held in registers:
@@ -21,6 +21,9 @@
 // Hydro fields are stored after D (the second application leaves them unchanged for
 // the layouts the host accepts).  Every face is evaluated once per warp; the only
 // redundant work is the 6 halo columns of each strip and 6 halo rows of each band.
+// Warp votes skip work whose result is known for the whole warp: the entropy-fix terms
+// without a transonic face, the momentum corrections where every cell is wet, the Exner
+// block where no cell of the two rows carries sediment (see the phases below).
 #pragma once
 #include <type_traits>
 
