@@ -152,9 +152,10 @@ cudaError_t launch_set_time(CflScratch* scr, double t0, cudaStream_t s) {
 
 template <class T>
 cudaError_t launch_roe_stage(const RoeArgs<T>& a, bool avg, cudaStream_t s) {
-    dim3 b(32, 8), g((a.nx + 31) / 32, (a.ny + 7) / 8);
-    if (avg) roe_stage_kernel<T, true><<<g, b, 0, s>>>(a);
-    else roe_stage_kernel<T, false><<<g, b, 0, s>>>(a);
+    const long long threads = 4LL * a.ny * a.nx;  // four threads per cell
+    const int g = (int)((threads + 255) / 256);
+    if (avg) roe_stage_kernel<T, true><<<g, 256, 0, s>>>(a);
+    else roe_stage_kernel<T, false><<<g, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 

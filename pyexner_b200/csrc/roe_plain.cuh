@@ -1,11 +1,11 @@
 // Plain Roe shallow-water step (no Exner): PyExner src/PyExner/solvers/kernels/roe.py
 // and src/PyExner/solvers/roe_solver.py.
 //
-// One thread per cell; each thread evaluates its four faces (every face is evaluated by
-// both of its cells).  Ring cells with boundary recipes recompute the update of their
-// donor cell instead of reading it, so the stage is one launch with no global
-// synchronisation.  The plain Roe configuration is small (258 x 258) and latency-bound;
-// the Roe-Exner stage is the one built for bandwidth.
+// Four threads per cell, one face each (every face is evaluated by both of its cells).
+// Ring cells with boundary recipes recompute the update of their donor cell instead of
+// reading it, so the stage is one launch with no global synchronisation.  The plain Roe
+// configuration is small (258 x 258) and latency-bound; the Roe-Exner stage is the one
+// built for bandwidth.
 #pragma once
 #include "pxb_device.cuh"
 
@@ -24,10 +24,12 @@ struct RoeArgs {
     int* err;
 };
 
-// Roe fluctuations with the wet/dry thrust and beta limiter (roe.py:32-249).
-template <class T, bool YF>
+// Roe fluctuations with the wet/dry thrust and beta limiter (roe.py:32-249).  YF (the
+// y-face orientation) is a runtime flag, so that the four threads of a cell, two on
+// x-faces and two on y-faces, run one code path.
+template <class T>
 __device__ __forceinline__ void roe_plain_face(T hi, T hui, T hvi, T zi, T ni, T hj, T huj, T hvj, T zj, T nj, T dx,
-                                               T P[3], T M[3]) {
+                                               const bool YF, T P[3], T M[3]) {
     const T DRY = T(DRY_TOL);
     hi = hi > DRY ? hi : T(0);
     hj = hj > DRY ? hj : T(0);
@@ -146,54 +148,70 @@ __device__ __forceinline__ void roe_plain_face(T hi, T hui, T hvi, T zi, T ni, T
 }
 
 // Update of cell (r, c) from its four faces (roe.py:251-315), order of roe.py:296-299.
+// Update of cell (r, c) by the four threads of its quad (adjacent lanes qbase..qbase+3):
+// thread q evaluates face q of the cell (0 east, 1 west, 2 south = row + 1, 3 north =
+// row - 1) and the sums run in that order, the scatter order of roe.py (east upwM, west
+// upwP, south upwM, north upwP).  One face per thread: the 66 k-cell configuration of
+// this path is latency-bound, and four threads per cell keep four times as many in
+// flight as one thread evaluating the four faces in turn.
 template <class T>
-__device__ __forceinline__ void roe_cell_update(const RoeArgs<T>& a, int r, int c, T dt, T out[3]) {
+__device__ __forceinline__ void roe_quad_update(const RoeArgs<T>& a, int r, int c, T dt, int q, unsigned qmask,
+                                                int qbase, T out[3]) {
     const long long p = a.pitch;
     const long long i = (long long)r * p + c;
-    const T h = a.h[i], hu = a.hu[i], hv = a.hv[i], z = a.z[i], n = a.n[i];
-    T f0 = 0, f1 = 0, f2 = 0, P[3], M[3];
-    if (c + 1 < a.nx) {
-        const long long j = i + 1;
-        roe_plain_face<T, false>(h, hu, hv, z, n, a.h[j], a.hu[j], a.hv[j], a.z[j], a.n[j], a.dx, P, M);
-        f0 = f0 + M[0]; f1 = f1 + M[1]; f2 = f2 + M[2];
+    const bool first = (q & 1) == 0;  // the cell is the face's i side (east, south faces)
+    const bool yf = q >= 2;
+    const bool has = q == 0 ? (c + 1 < a.nx) : q == 1 ? (c >= 1) : q == 2 ? (r + 1 < a.ny) : (r >= 1);
+    const long long j = q == 0 ? i + 1 : q == 1 ? i - 1 : q == 2 ? i + p : i - p;
+    T v[3] = {T(0), T(0), T(0)};
+    if (has) {
+        const long long ii = first ? i : j, jj = first ? j : i;
+        T P[3], M[3];
+        roe_plain_face<T>(a.h[ii], a.hu[ii], a.hv[ii], a.z[ii], a.n[ii], a.h[jj], a.hu[jj], a.hv[jj], a.z[jj], a.n[jj],
+                          a.dx, yf, P, M);
+#pragma unroll
+        for (int m = 0; m < 3; ++m) v[m] = first ? M[m] : P[m];
     }
-    if (c >= 1) {
-        const long long j = i - 1;
-        roe_plain_face<T, false>(a.h[j], a.hu[j], a.hv[j], a.z[j], a.n[j], h, hu, hv, z, n, a.dx, P, M);
-        f0 = f0 + P[0]; f1 = f1 + P[1]; f2 = f2 + P[2];
+    T f[3] = {T(0), T(0), T(0)};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const bool hk = __shfl_sync(qmask, (int)has, qbase + k) != 0;
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            const T vk = __shfl_sync(qmask, v[m], qbase + k);
+            if (hk) f[m] = f[m] + vk;
+        }
     }
-    if (r + 1 < a.ny) {
-        const long long j = i + p;
-        roe_plain_face<T, true>(h, hu, hv, z, n, a.h[j], a.hu[j], a.hv[j], a.z[j], a.n[j], a.dx, P, M);
-        f0 = f0 + M[0]; f1 = f1 + M[1]; f2 = f2 + M[2];
-    }
-    if (r >= 1) {
-        const long long j = i - p;
-        roe_plain_face<T, true>(a.h[j], a.hu[j], a.hv[j], a.z[j], a.n[j], h, hu, hv, z, n, a.dx, P, M);
-        f0 = f0 + P[0]; f1 = f1 + P[1]; f2 = f2 + P[2];
-    }
-    out[0] = h - dt * f0 / a.dx;
-    out[1] = hu - dt * f1 / a.dx;
-    out[2] = hv - dt * f2 / a.dx;
+    out[0] = a.h[i] - dt * f[0] / a.dx;
+    out[1] = a.hu[i] - dt * f[1] / a.dx;
+    out[2] = a.hv[i] - dt * f[2] / a.dx;
 }
 
+// One stage; four threads per cell.  Ring cells with boundary recipes recompute the
+// update of their donor cell instead of reading it, so the stage is one launch with no
+// global synchronisation.
 template <class T, bool AVG>
 __global__ void __launch_bounds__(256) roe_stage_kernel(const RoeArgs<T> a) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    const int r = blockIdx.y * blockDim.y + threadIdx.y;
-    if (r >= a.ny || c >= a.nx) return;
+    const int lane = threadIdx.x & 31;
+    const int qbase = lane & ~3;
+    const unsigned qmask = 0xFu << qbase;
+    const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long cell = tid >> 2;
+    const int q = (int)(tid & 3);
+    if (cell >= (long long)a.ny * a.nx) return;  // whole quads leave together
+    const int r = (int)(cell / a.nx), c = (int)(cell - (long long)r * a.nx);
     const T dt = *a.dt;
     const long long i = (long long)r * a.pitch + c;
     T u[3];
-    roe_cell_update(a, r, c, dt, u);
+    roe_quad_update(a, r, c, dt, q, qmask, qbase, u);
     const bool on_ring = (r == 0) || (r == a.ny - 1) || (c == 0) || (c == a.nx - 1);
     T zo = a.z[i], no = a.n[i];
-    if (on_ring && a.ring != nullptr) {
+    if (on_ring && a.ring != nullptr) {  // the same for the four threads of the quad
         const pxb_ring_recipe& rc = a.ring[ring_slot(r, c, a.ny, a.nx)];
         if (rc.flags & 1u) {  // Roe handlers write h, z and n from the same donor
             T d[3];
             const int rr = r + rc.h_dy, cc = c + rc.h_dx;
-            roe_cell_update(a, rr, cc, dt, d);
+            roe_quad_update(a, rr, cc, dt, q, qmask, qbase, d);
             u[0] = d[0];
             const long long j = (long long)rr * a.pitch + cc;
             zo = a.z[j];
@@ -205,12 +223,13 @@ __global__ void __launch_bounds__(256) roe_stage_kernel(const RoeArgs<T> a) {
                 u[2] = T(rc.m[1]);
             } else {
                 T d[3];
-                roe_cell_update(a, r + rc.m_dy, c + rc.m_dx, dt, d);
+                roe_quad_update(a, r + rc.m_dy, c + rc.m_dx, dt, q, qmask, qbase, d);
                 u[1] = T(rc.m[0]) * d[1] + T(rc.m[1]) * d[2];
                 u[2] = T(rc.m[2]) * d[1] + T(rc.m[3]) * d[2];
             }
         }
     }
+    if (q != 0) return;  // the quad's first thread writes the cell
     if (AVG) {
         u[0] = T(0.5) * a.ah[i] + T(0.5) * u[0];
         u[1] = T(0.5) * a.ahu[i] + T(0.5) * u[1];
