@@ -21,7 +21,7 @@ Reported:
   accuracy   rel-L1 of h and z+z_b, float32 vs float64 after the accuracy run;
   cpu_baseline  the float64 C/OpenMP oracle (all host threads) on a 512 x 512 sample of
              the same generator, about 10 s of CPU work;
-  plain_roe  configuration 1: the plain Roe dam-break (256^2, float64, SSPRK2, 200 steps)
+  plain_roe  the plain Roe dam-break (256^2, float64, SSPRK2, 200 steps)
              and the NumPy oracle on the host for 10 steps of it;
   transport_case  the same case started at u = 1 m/s (Shields number about 0.15, bedload
              in every cell, so the stage kernel's sediment-free fast path never fires);
@@ -376,7 +376,7 @@ def ensemble_run(count, steps, seed=0):
 
 
 def plain_roe_run(steps=200, cpu_steps=10):
-    """Configuration 1: the plain Roe dam-break, 256 x 256 cells, float64, SSPRK2, 200
+    """The plain Roe dam-break, 256 x 256 cells, float64, SSPRK2, 200
     steps through ``run_steps`` (graph replay), and the float64 NumPy oracle on the host
     for ``cpu_steps`` steps of the same case (single thread)."""
     import torch
@@ -483,6 +483,22 @@ def profile_sequence(args):
     from pyexner_b200.integrators import check_state
 
     build.build()
+    if args.profile_case == "roe":  # the plain Roe dam-break (256^2, float64)
+        from pyexner_b200 import BoundaryManager, RoeState, cases, create_solver_bundle
+
+        c = cases.dambreak_roe(256)
+        params = dict(flux_scheme="Roe", boundaries=c["params"]["boundaries"])
+        bm = BoundaryManager(params, c["X"], c["Y"])
+        st = RoeState.from_numpy(c["arrs"], torch.float64)
+        bundle = create_solver_bundle("Roe")
+        cfg = bundle.config(st, None, bm, c["dx"], params)
+        mask = bundle.mask_fn(st)
+        st = bundle.init_fn(st, mask, cfg)
+        run_steps(st, mask, cfg, "SSPRK2", max(1, args.warmup), 0.5, log_dt=False)
+        torch.cuda.synchronize()
+        if not bool(torch.isfinite(st.h).all()):
+            raise SystemExit("plain Roe profile case: non-finite depth")
+        return
     dt = torch.float32 if args.dtype == "f32" else torch.float64
     c, bundle, cfg, mask, st = build_case(args.n, dt, "cuda")
     run_steps(st, mask, cfg, "SSPRK2", max(1, args.warmup), 0.5)
@@ -508,6 +524,8 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="short fixed sequence for ncu: build the case, run --warmup SSPRK2 steps, exit")
     ap.add_argument("--dtype", default="f32", choices=["f32", "f64"])
+    ap.add_argument("--profile-case", default="gaussian", choices=["gaussian", "roe"],
+                    help="case of --profile: the Gaussian-bed Roe-Exner grid or the plain Roe dam-break")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)

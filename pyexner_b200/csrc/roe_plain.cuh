@@ -187,14 +187,66 @@ __device__ __forceinline__ void roe_quad_update(const RoeArgs<T>& a, int r, int 
     out[2] = a.hv[i] - dt * f[2] / a.dx;
 }
 
+// The larger of the two speeds of compute_dt for plain Roe (roe.py:13-30) at one cell,
+// |u| + c + VEL_TOL and |v| + c + VEL_TOL, as an IEEE bit pattern (speeds are positive or
+// NaN, so unsigned order is float order and NaN wins).
+template <class T>
+__device__ __forceinline__ unsigned long long roe_cell_speed_bits(T h0, T hu0, T hv0) {
+    const bool wet = h0 > T(DRY_TOL);
+    const T h = wet ? h0 : T(0);
+    const T hv = wet ? hv0 : T(0);
+    const T hu = wet ? hu0 : T(0);
+    const T u = hu / (h + T(DRY_TOL));
+    const T v = hv / (h + T(DRY_TOL));
+    const T cc = d_sqrt(T(G_ACC) * h);
+    const T sx = fabs(u) + cc + T(VEL_TOL);
+    const T sy = fabs(v) + cc + T(VEL_TOL);
+    const unsigned long long bx = speed_bits(sx), by = speed_bits(sy);
+    return bx > by ? bx : by;
+}
+
+// Max over the launch of the threads' speed bits (warp max, block max through shared
+// memory, one atomicMax per block), and the last block to finish turns it into
+// dt = cfl * dx / smax (no floor), logs it and resets the accumulator.  Every thread of
+// every block calls it once, at its end.
+template <class T>
+__device__ __forceinline__ void roe_dt_reduce(unsigned long long best, CflScratch* scr, T cfl, T dx, T* dt_out,
+                                              T* dt_log) {
+    const int lane = threadIdx.x & 31;
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long other = __shfl_xor_sync(FULL, best, o);
+        best = other > best ? other : best;
+    }
+    __shared__ unsigned long long wmax[32];
+    if (lane == 0) wmax[threadIdx.x >> 5] = best;
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    for (int w = 1; w < (int)((blockDim.x + 31) >> 5); ++w) best = wmax[w] > best ? wmax[w] : best;
+    if (best != 0ull) atomicMax(&scr->maxbits, best);
+    __threadfence();  // the block's maximum before its ticket
+    const unsigned int ticket = atomicAdd(&scr->done, 1u);
+    if (ticket != gridDim.x - 1) return;
+    __threadfence();
+    const unsigned long long bits = atomicAdd(&scr->maxbits, 0ull);
+    const T smax = bits_speed(bits, T(0));
+    const T dt = cfl * (dx / smax);
+    *dt_out = dt;
+    if (dt_log) dt_log[scr->step] = dt;
+    scr->step += 1;
+    if (!d_isfinite(dt)) scr->err |= 2;
+    scr->maxbits = 0ull;
+    scr->done = 0u;
+    __threadfence();
+}
+
 // One stage; four threads per cell.  Ring cells with boundary recipes recompute the
 // update of their donor cell instead of reading it, so the stage is one launch with no
 // global synchronisation.
-// Resident 256-thread blocks per SM the stage is register-limited to (tuning knob): 3
-// (80 registers, some spills) measured 6 % faster than 2 and than the compiler's 96
-// registers on the 256^2 dam break
+// Resident 256-thread blocks per SM the stage is register-limited to (tuning knob): 4
+// (64 registers, a few hundred bytes of spills) runs the 256^2 dam break's 266 k threads
+// in 2 waves instead of 2.3, 3 % faster than 3 (80 registers) and 8 % faster than 2.
 #ifndef PXB_ROE_MIN_BLOCKS
-#define PXB_ROE_MIN_BLOCKS 3
+#define PXB_ROE_MIN_BLOCKS 4
 #endif
 
 template <class T, bool AVG>
@@ -209,31 +261,57 @@ __global__ void __launch_bounds__(256, PXB_ROE_MIN_BLOCKS) roe_stage_kernel(cons
     const int r = (int)(cell / a.nx), c = (int)(cell - (long long)r * a.nx);
     const T dt = *a.dt;
     const long long i = (long long)r * a.pitch + c;
-    T u[3];
-    roe_quad_update(a, r, c, dt, q, qmask, qbase, u);
     const bool on_ring = (r == 0) || (r == a.ny - 1) || (c == 0) || (c == a.nx - 1);
-    T zo = a.z[i], no = a.n[i];
-    if (on_ring && a.ring != nullptr) {  // the same for the four threads of the quad
+    // The same for the four threads of the quad: Roe handlers write h, z and n from one
+    // donor (flags bit 0) and the momentum from another (bit 1: a 2x2 map of the donor's,
+    // or constants with bit 2).
+    unsigned flags = 0u;
+    int hdy = 0, hdx = 0, mdy = 0, mdx = 0;
+    T m0 = T(0), m1 = T(0), m2 = T(0), m3 = T(0);
+    if (on_ring && a.ring != nullptr) {
         const pxb_ring_recipe& rc = a.ring[ring_slot(r, c, a.ny, a.nx)];
-        if (rc.flags & 1u) {  // Roe handlers write h, z and n from the same donor
-            T d[3];
-            const int rr = r + rc.h_dy, cc = c + rc.h_dx;
-            roe_quad_update(a, rr, cc, dt, q, qmask, qbase, d);
-            u[0] = d[0];
-            const long long j = (long long)rr * a.pitch + cc;
-            zo = a.z[j];
-            no = a.n[j];
+        flags = rc.flags;
+        hdy = rc.h_dy, hdx = rc.h_dx, mdy = rc.m_dy, mdx = rc.m_dx;
+        m0 = T(rc.m[0]), m1 = T(rc.m[1]), m2 = T(rc.m[2]), m3 = T(rc.m[3]);
+    }
+    // Updates evaluated in turn by one inlined copy of the quad update: the cell itself
+    // (unless both of its parts come from donors), the h donor, the momentum donor.
+    T u[3] = {T(0), T(0), T(0)}, dh[3] = {T(0), T(0), T(0)}, dm[3] = {T(0), T(0), T(0)};
+#pragma unroll 1
+    for (int pass = 0; pass < 3; ++pass) {
+        int rr = r, cc = c;
+        if (pass == 0 && (flags & 3u) == 3u) continue;
+        if (pass == 1) {
+            if (!(flags & 1u)) continue;
+            rr = r + hdy, cc = c + hdx;
         }
-        if (rc.flags & 2u) {
-            if (rc.flags & 4u) {
-                u[1] = T(rc.m[0]);
-                u[2] = T(rc.m[1]);
-            } else {
-                T d[3];
-                roe_quad_update(a, r + rc.m_dy, c + rc.m_dx, dt, q, qmask, qbase, d);
-                u[1] = T(rc.m[0]) * d[1] + T(rc.m[1]) * d[2];
-                u[2] = T(rc.m[2]) * d[1] + T(rc.m[3]) * d[2];
-            }
+        if (pass == 2) {
+            if (!(flags & 2u) || (flags & 4u)) continue;
+            rr = r + mdy, cc = c + mdx;
+        }
+        T d[3];
+        roe_quad_update(a, rr, cc, dt, q, qmask, qbase, d);
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            u[m] = pass == 0 ? d[m] : u[m];
+            dh[m] = pass == 1 ? d[m] : dh[m];
+            dm[m] = pass == 2 ? d[m] : dm[m];
+        }
+    }
+    T zo = a.z[i], no = a.n[i];
+    if (flags & 1u) {
+        u[0] = dh[0];
+        const long long j = (long long)(r + hdy) * a.pitch + (c + hdx);
+        zo = a.z[j];
+        no = a.n[j];
+    }
+    if (flags & 2u) {
+        if (flags & 4u) {
+            u[1] = m0;
+            u[2] = m1;
+        } else {
+            u[1] = m0 * dm[1] + m1 * dm[2];
+            u[2] = m2 * dm[1] + m3 * dm[2];
         }
     }
     if (q != 0) return;  // the quad's first thread writes the cell
@@ -258,54 +336,15 @@ __global__ void __launch_bounds__(256, PXB_ROE_MIN_BLOCKS) roe_stage_kernel(cons
 // (|u| + c + VEL_TOL) and (|v| + c + VEL_TOL); no floor.
 template <class T>
 __global__ void __launch_bounds__(256) roe_cfl_kernel(const CflArgs<T> a) {
-    const int lane = threadIdx.x & 31;
     unsigned long long best = 0ull;
     const long long ncell = (long long)a.ny * a.nx;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < ncell; k += (long long)gridDim.x * blockDim.x) {
         const int r = (int)(k / a.nx), c = (int)(k - (long long)r * a.nx);
         const long long i = (long long)r * a.pitch + c;
-        const bool wet = a.h[i] > T(DRY_TOL);
-        const T h = wet ? a.h[i] : T(0);
-        const T hv = wet ? a.hv[i] : T(0);
-        const T hu = wet ? a.hu[i] : T(0);
-        const T u = hu / (h + T(DRY_TOL));
-        const T v = hv / (h + T(DRY_TOL));
-        const T cc = d_sqrt(T(G_ACC) * h);
-        const T sx = fabs(u) + cc + T(VEL_TOL);
-        const T sy = fabs(v) + cc + T(VEL_TOL);
-        const unsigned long long bx = speed_bits(sx), by = speed_bits(sy);
-        best = bx > best ? bx : best;
-        best = by > best ? by : best;
+        const unsigned long long b = roe_cell_speed_bits(a.h[i], a.hu[i], a.hv[i]);
+        best = b > best ? b : best;
     }
-    for (int o = 16; o > 0; o >>= 1) {
-        const unsigned long long other = __shfl_xor_sync(FULL, best, o);
-        best = other > best ? other : best;
-    }
-    if (lane == 0) {
-        if (best != 0ull) atomicMax(&a.scr->maxbits, best);
-        __threadfence();
-    }
-    __shared__ bool last;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const unsigned int ticket = atomicAdd(&a.scr->done, 1u);
-        last = (ticket == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (last && threadIdx.x == 0) {
-        __threadfence();
-        const unsigned long long bits = atomicAdd(&a.scr->maxbits, 0ull);
-        const T smax = bits_speed(bits, T(0));
-        const T dt = a.cfl * (a.dx / smax);
-        *a.dt_out = dt;
-        if (a.dt_log) a.dt_log[a.scr->step] = dt;
-        a.scr->step += 1;
-        if (!d_isfinite(dt)) a.scr->err |= 2;
-        a.scr->maxbits = 0ull;
-        a.scr->done = 0u;
-        __threadfence();
-    }
+    roe_dt_reduce<T>(best, a.scr, a.cfl, a.dx, a.dt_out, a.dt_log);
 }
 
 }  // namespace pxb

@@ -183,6 +183,37 @@ def test_roe_dambreak_200_steps():
         assert l1_rel(got[f], ost[f]) <= 1e-10, f
 
 
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "f32"])
+@pytest.mark.parametrize("scheme", ["FE", "SSPRK2"])
+@pytest.mark.parametrize("case", ROE_CASES, ids=[c[0] for c in ROE_CASES])
+def test_roe_run_matches_step_by_step(request, case, scheme, dtype):
+    """run_steps computes each next dt inside the last stage of a step (the last step
+    computes none); the states and dts are those of compute_dt_fn + step_fn called step by
+    step, bit for bit, for odd and even step counts of both schemes."""
+    from pyexner_b200 import run_steps
+    from pyexner_b200.integrators import _ssprk2_step
+
+    name, (ny, nx), _regime, bcname = case
+    d = np.load(request.config.rootpath / "tests" / "golden" / f"roe_{name}.npz")
+    X, Y = grid_coords(ny, nx)
+    arrs = {f: d[f"in_{f}"] for f in ("h", "hu", "hv", "z", "n")}
+    bundle, cfg, mask, st = device_roe(arrs, ROE_BC_SPECS[bcname](ny, nx), X, Y, dtype, float(d["dx"]))
+    for n in (1, 2, 3, 4, 7):
+        s = st.clone()
+        dts = run_steps(s, mask, cfg, scheme, n, 0.5).cpu().numpy()
+        ref = st.clone()
+        ref_dts = []
+        for _ in range(n):
+            dt = bundle.compute_dt_fn(ref, 0.5, mask, cfg)
+            ref_dts.append(float(dt))
+            ref = _ssprk2_step(bundle, ref, 0.0, dt, mask, cfg) if scheme == "SSPRK2" else \
+                bundle.step_fn(ref, 0.0, dt, mask, cfg)
+        assert np.array_equal(dts, np.array(ref_dts, dtype=dts.dtype)), (n, dts, ref_dts)
+        got, want = s.to_numpy(), ref.to_numpy()
+        for f in ("h", "hu", "hv", "z", "n"):
+            assert np.array_equal(got[f], want[f]), (n, f)
+
+
 def test_nonfinite_state_is_reported():
     from pyexner_b200 import run_steps
     from pyexner_b200._lib import ERR_NONFINITE, PxbError
