@@ -174,25 +174,22 @@ __global__ void __launch_bounds__(256) re_cfl_kernel(const CflArgs<T> a) {
         if (lane == 0) next = atomicAdd(&a.scr->cfl_queue, 1u);
         item = nw + (int)__shfl_sync(FULL, next, 0);
     }
-    // warp max, one atomic per warp
+    // warp max, block max through shared memory, one atomic and one fence per block
     for (int o = 16; o > 0; o >>= 1) {
         const unsigned long long other = __shfl_xor_sync(FULL, best, o);
         best = other > best ? other : best;
     }
-    if (lane == 0) {
-        if (best != 0ull) atomicMax(&a.scr->maxbits, best);
-        __threadfence();
-    }
+    __shared__ unsigned long long wmax[8];
+    if (lane == 0) wmax[threadIdx.x >> 5] = best;
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+#pragma unroll
+    for (int w = 1; w < 8; ++w) best = wmax[w] > best ? wmax[w] : best;
+    if (best != 0ull) atomicMax(&a.scr->maxbits, best);
+    __threadfence();  // the block's maximum before its ticket
     // last block finalises
-    __shared__ bool last;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const unsigned int ticket = atomicAdd(&a.scr->done, 1u);
-        last = (ticket == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (last && threadIdx.x == 0) {
+    const unsigned int ticket = atomicAdd(&a.scr->done, 1u);
+    if (ticket == gridDim.x - 1) {
         __threadfence();
         const unsigned long long bits = atomicAdd(&a.scr->maxbits, 0ull);
         const T smax = bits_speed(bits, T(0));
