@@ -855,7 +855,9 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
         for (; r < steady0; ++r) iterate(r, std::false_type{});
         PXB_UNROLL(PXB_STAGE_UNROLL)
         for (; r < steady1; ++r) iterate(r, std::true_type{});
-        for (; r < L1 + 5; ++r) iterate(r, std::false_type{});
+        // drain until phase G has stored the band's last row (p = R1 - 1 at r = R1 + 4);
+        // later iterations would only advance the halo rows below the band
+        for (; r < R1 + 5; ++r) iterate(r, std::false_type{});
         cp_async_wait<0>();  // the buffers are reused by the next item
     }
 }
