@@ -299,6 +299,11 @@ struct Geometry {
     int band_rows = 0, nstrips = 0, nbands = 0, grid = 0;
 };
 
+// Tallest band of the stage kernel's default geometry (tuning knob; float32 Gaussian bed:
+// 160 and 192 measured alike at 8192^2, 160 ahead of 192 at 4096^2)
+#ifndef PXB_STAGE_MAX_ROWS
+#define PXB_STAGE_MAX_ROWS 176
+#endif
 #ifndef PXB_CFL_ITEMS_PER_WARP
 #define PXB_CFL_ITEMS_PER_WARP 2
 #endif
@@ -312,11 +317,15 @@ Geometry stage_geometry(int ny, int nx, int esize, int resident_warps, int want_
     g.nstrips = std::max(1, (nx - 3 + sout - 1) / sout);
     int rows = want_rows;
     if (rows <= 0) {
-        // enough bands to give every resident warp an item, but no band taller than 128
-        // rows: on large grids several waves of shorter bands keep the concurrently active
-        // items close together in memory (halo rows and columns shared through L2)
-        const int target_bands = std::max(1, resident_warps / pxb_stage_items_per_band(g.nstrips));
-        rows = std::max(8, std::min(128, (ny - 1 + target_bands - 1) / target_bands));
+        // k rounds of items, each with about one item per resident warp (the work queue
+        // hands out the items beyond the first), for the smallest k whose bands are at most
+        // PXB_STAGE_MAX_ROWS tall: a whole number of rounds leaves no partial last round
+        // with idle SMs, and on large grids several rounds of shorter bands keep the
+        // concurrently active items close together in memory (halos shared through L2)
+        const int ipb = pxb_stage_items_per_band(g.nstrips), span = ny - 1;
+        int k = 1, bands = std::max(1, resident_warps / ipb);
+        while ((span + bands - 1) / bands > PXB_STAGE_MAX_ROWS) bands = std::max(1, ++k * resident_warps / ipb);
+        rows = std::max(8, (span + bands - 1) / bands);
     }
     g.band_rows = rows;
     g.nbands = std::max(1, (ny - 1 + rows - 1) / rows);
