@@ -1328,7 +1328,7 @@ int ens_run_impl(pxb_re_ens* E, int nsteps, int scheme, double cfl, void* dt_log
 // Candidate band heights timed on stage 1 (a -> b) of the current states; keeps the fastest.
 template <class T>
 int ens_autotune_impl(pxb_re_ens* E, cudaStream_t s, int32_t* out) {
-    static const int cand[] = {8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256};
+    static const int cand[] = {8, 12, 16, 24, 32, 48, 64, 96, 128, 160, 192, 256};
     int st = ens_build_cfl_tables<T>(E, 0.5, nullptr);
     if (st != PXB_OK) return st;
     st = ens_cfl_launch<T>(E, 0, s);  // a dt to run the stage with (the states are not touched)
