@@ -5,8 +5,9 @@
 // min over active faces of dx / speed_f equals dx / max_f speed_f exactly (division by
 // a positive number is monotone under round-to-nearest), so the kernel reduces the
 // maximum speed: a warp-level max of the IEEE bit patterns (speeds are >= 0 or NaN, so
-// unsigned order is float order and NaN wins like jnp.min's NaN), one 64-bit atomicMax
-// per warp, and the last block to finish turns it into dt = max(cfl * dx / smax, 1e-6),
+// unsigned order is float order and NaN wins like jnp.min's NaN), a block max through
+// shared memory, one 64-bit atomicMax per block, and the last block to finish turns it
+// into dt = max(cfl * dx / smax, 1e-6),
 // resets the accumulator and logs dt.  Deterministic and free of host round trips.
 //
 // Work layout: a warp covers 32 columns and the 31 x-faces between them (strips overlap
