@@ -51,7 +51,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "cell-updates/s Roe-Exner SSPRK2 FP32 vs FP64 at stated L1 err; % HBM peak"
 UNIT = "cell-updates/s"
-# algorithmic words per cell per launch (Measurement)
+# algorithmic words per cell per launch of the stage / CFL kernels
 WORDS_STAGE1 = 10   # reads h hu hv z_b z n_b, writes h hu hv z_b
 WORDS_STAGE2 = 16   # reads h hu hv z_b z n_b + u^n h hu hv z_b G, writes h hu hv z_b G
 WORDS_CFL = 4       # reads h hu hv G
@@ -165,6 +165,18 @@ def max_over_ranks(sec, world, device):
 
     t = torch.tensor([float(sec)], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t)
+
+
+def sum_over_ranks(x, world, device):
+    """Sum of a per-rank count (one all-reduce of a timing-side scalar)."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t)
 
 
@@ -311,41 +323,71 @@ def e2e_run(n, dtype, steps, warmup):
     return sec, h2d, d2h
 
 
-def accuracy_run(n, steps):
-    """rel-L1 (h, total bed) of float32 vs float64 after ``steps`` SSPRK2 steps."""
+def gpu_run_with_budget(n, dtype, steps):
+    """``steps`` SSPRK2 steps of the Gaussian-bed case at n x n on the GPU with the volume
+    budget on; returns the final state and the budget closure (volume(end) - volume(start)
+    + outflow, relative to the start volume, for water and sediment)."""
     import torch
 
-    from pyexner_b200 import run_steps
+    from pyexner_b200 import new_budget, outflow, run_steps, volume
+
+    c, bundle, cfg, mask, st = build_case(n, dtype, "cuda")
+    w0, z0 = volume(st, mask, cfg)
+    bud = new_budget()
+    run_steps(st, mask, cfg, "SSPRK2", steps, 0.5, budget=bud, log_dt=False)
+    torch.cuda.synchronize()
+    w1, z1 = volume(st, mask, cfg)
+    ow, oz = outflow(bud)
+    return st.to_numpy(), {"water_outflow_m3": ow, "sediment_outflow_m3": oz,
+                           "water_closure_rel": (w1 - w0 + ow) / w0, "sediment_closure_rel": (z1 - z0 + oz) / z0}
+
+
+def accuracy_run(n, steps, n_oracle, oracle_proc, oracle_path):
+    """Float32 against float64 on the GPU at n x n after ``steps`` SSPRK2 steps, and at
+    n_oracle x n_oracle both GPU precisions against the float64 C oracle (run by the
+    spawned ``oracle_proc``), each with its volume-budget closure."""
+    import torch
 
     res = {}
     for dt in (torch.float32, torch.float64):
-        c, bundle, cfg, mask, st = build_case(n, dt, "cuda")
-        t0 = time.time()
-        run_steps(st, mask, cfg, "SSPRK2", steps, 0.5)
-        torch.cuda.synchronize()
-        res[dt] = (st.to_numpy(), time.time() - t0)
-    a, b = res[torch.float32][0], res[torch.float64][0]
-    s = (slice(1, -1), slice(1, -1))
+        res[dt] = gpu_run_with_budget(n, dt, steps)
+    out = {"steps": steps, "n": n, "fp32_vs_fp64_gpu": errors_vs(res[torch.float32][0], res[torch.float64][0]),
+           "budget_fp32": res[torch.float32][1], "budget_fp64": res[torch.float64][1]}
+    out["h_rel_l1"] = out["fp32_vs_fp64_gpu"]["h"]["rel_l1"]
+    out["bed_rel_l1"] = out["fp32_vs_fp64_gpu"]["bed"]["rel_l1"]
+    if oracle_proc is not None:
+        g32, _ = gpu_run_with_budget(n_oracle, torch.float32, steps)
+        g64, _ = gpu_run_with_budget(n_oracle, torch.float64, steps)
+        oracle_proc.join()
+        if oracle_proc.exitcode == 0 and os.path.exists(oracle_path):
+            ref = dict(np.load(oracle_path))
+            e32, e64 = errors_vs(g32, ref), errors_vs(g64, ref)
+            out["vs_oracle"] = {"vs": "oracle_f64", "n": n_oracle, "steps": steps,
+                                "oracle_seconds": float(ref["sec"]), "oracle_cores": _cores(),
+                                "fp32": e32, "fp64": e64,
+                                "fp32_h_bed_rel_l1_le_1e-5": bool(e32["h"]["rel_l1"] <= 1e-5 and
+                                                                  e32["bed"]["rel_l1"] <= 1e-5)}
+        else:
+            out["vs_oracle"] = {"error": f"oracle process exit code {oracle_proc.exitcode}"}
+    return out
 
-    def l1(x, y):
-        return float(np.sum(np.abs(x - y)) / np.sum(np.abs(y)))
 
-    return {"steps": steps, "n": n, "h_rel_l1": l1(a["h"][s], b["h"][s]),
-            "bed_rel_l1": l1((a["z"] + a["z_b"])[s], (b["z"] + b["z_b"])[s]),
-            "hu_rel_l1": l1(a["hu"][s], b["hu"][s])}
-
-
-def ensemble_run(count, steps, seed=0):
+def ensemble_run(count, steps, seed=0, world=1, rank=0):
     """The ragged ensemble: ``count`` dam breaks of random sizes advanced together, one
-    launch per phase for all members, every member with its own dt."""
+    launch per phase for all members, every member with its own dt.  With several ranks
+    (replicas) the members are split over the ranks by ``partition_members`` and each rank
+    advances its share; the whole-job rate is the sum of the ranks' cells over the slowest
+    rank's time (two all-reduces of timing scalars, no data-path collective)."""
     import torch
 
     from pyexner_b200 import BoundaryManager, RoeExnerState
     from pyexner_b200.boundaries import index_coords
     from pyexner_b200.cases import ensemble_case, seds_matrix
-    from pyexner_b200.ensemble import Ensemble
+    from pyexner_b200.ensemble import Ensemble, partition_members
 
     members, erosion = ensemble_case(count, seed)
+    mine = partition_members([m["shape"][0] * m["shape"][1] for m in members], world)[rank]
+    members = [members[k] for k in mine]
     seds = seds_matrix(erosion)
     mbs = []
     for m in members:
@@ -369,8 +411,10 @@ def ensemble_run(count, steps, seed=0):
     ens.check()
     cells = ens.cells()
     d = dts.double()
+    cells_all, sec = sum_over_ranks(cells, world, "cuda"), max_over_ranks(sec, world, "cuda")
     return {"workload": f"roe_exner_ragged_ensemble_{count}_dambreaks_128-1024_mpm_ssprk2_f32",
-            "members": count, "cells": cells, "steps": steps, "value": cells * steps / sec, "unit": UNIT,
+            "members": count, "members_this_rank": len(mine), "cells": cells_all, "steps": steps,
+            "value": cells_all * steps / sec, "unit": UNIT, "scaling": "strong" if world > 1 else None,
             "ms_per_step": 1e3 * sec / steps, "band_rows": rows, "launches_per_step": 4,
             "dt_range": [float(d.min()), float(d.max())], "l2": "state ~1.1 GB, larger than L2"}
 
@@ -415,7 +459,7 @@ def plain_roe_run(steps=200, cpu_steps=10):
                            "sample": f"{cpu_steps} SSPRK2 steps of the same case, float64 NumPy oracle"}}
 
 
-def _oracle_case(n):
+def _oracle_case(n, dtype=np.float64):
     from oracle import boundaries as OB
     from oracle import c_oracle as CO
     from pyexner_b200 import cases
@@ -426,54 +470,93 @@ def _oracle_case(n):
     st["n_b"] = np.zeros_like(st["h"])
     st["seds"] = c["seds"]
     mask = OB.roe_exner_mask(st["z"].copy(), bcs.boundary_mask)
-    st = CO.init(st, mask, bcs, True, c["dx"])
+    st = CO.init(st, mask, bcs, True, c["dx"], dtype=dtype)
     return c, bcs, st, mask
 
 
-def cpu_oracle_sample(n=512, budget_s=10.0, min_steps=3):
-    """Float64 C/OpenMP oracle (all host threads) on the same generator at n x n,
-    SSPRK2 steps until ``budget_s`` seconds of CPU work."""
+def _cores():
+    return int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+
+
+def cpu_oracle_sample(n=2048, budget_s=10.0, min_steps=3, dtype=np.float32):
+    """The C/OpenMP restatement of the reference step (all host threads) on the
+    workload itself, SSPRK2 steps until ``budget_s`` seconds of CPU work."""
     from oracle import c_oracle as CO
 
-    c, bcs, st, mask = _oracle_case(n)
-    CO.run_roe_exner(st, mask, bcs, True, c["dx"], 0.5, 1, "SSPRK2")  # warm-up
+    c, bcs, st, mask = _oracle_case(n, dtype)
+    CO.run_roe_exner(st, mask, bcs, True, c["dx"], 0.5, 1, "SSPRK2", dtype=dtype)  # warm-up
     steps, sec = 0, 0.0
     while sec < budget_s or steps < min_steps:
         t0 = time.perf_counter()
-        st, _ = CO.run_roe_exner(st, mask, bcs, True, c["dx"], 0.5, 1, "SSPRK2")
+        st, _ = CO.run_roe_exner(st, mask, bcs, True, c["dx"], 0.5, 1, "SSPRK2", dtype=dtype)
         sec += time.perf_counter() - t0
         steps += 1
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return n * n * steps / sec, cores, (f"{n}x{n} Gaussian-bed case (same generator), {steps} SSPRK2 steps, "
-                                        f"float64 C/OpenMP restatement of the reference step, {cores} threads")
+    prec = "float32" if dtype == np.float32 else "float64"
+    return n * n * steps / sec, _cores(), (f"{n}x{n} Gaussian-bed case (the workload), {steps} SSPRK2 steps, "
+                                           f"{prec} C/OpenMP restatement of the reference step, {_cores()} threads")
 
 
 def reference_arm(args):
-    """The reference's algorithm on the host cores: the float64 C/OpenMP restatement of
-    PyExner's step (JAX, which runs the reference itself, is not installed here), on a
-    512 x 512 sample of the same workload; one timed step = one SSPRK2 step."""
+    """The reference's algorithm on the host cores, on the workload itself (2048 x 2048):
+    the C/OpenMP restatement of PyExner's step (JAX, which runs the reference itself, is
+    not installed here) in float32, the precision the reference ships (its state is
+    float32), with all host threads; one timed step = one SSPRK2 step.  The float64 build
+    of the same restatement (the oracle) is timed beside it on a few steps."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from oracle import c_oracle as CO
 
-    n = 512
-    c, bcs, st, mask = _oracle_case(n)
-    st, _ = CO.run_roe_exner(st, mask, bcs, True, c["dx"], 0.5, max(1, args.warmup), "SSPRK2")
+    n = args.n
+    c, bcs, st, mask = _oracle_case(n, np.float32)
+    st, _ = CO.run_roe_exner(st, mask, bcs, True, c["dx"], 0.5, max(1, args.warmup), "SSPRK2", dtype=np.float32)
     t0 = time.perf_counter()
-    st, _ = CO.run_roe_exner(st, mask, bcs, True, c["dx"], 0.5, args.steps, "SSPRK2")
+    st, _ = CO.run_roe_exner(st, mask, bcs, True, c["dx"], 0.5, args.steps, "SSPRK2", dtype=np.float32)
     sec = time.perf_counter() - t0
     v = n * n * args.steps / sec
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    sample = f"{n}x{n} sample of the Gaussian-bed case, {args.steps} SSPRK2 steps, float64, {cores} threads"
+    steps64 = max(2, args.steps // 5)
+    c64, bcs64, st64, mask64 = _oracle_case(n, np.float64)
+    CO.run_roe_exner(st64, mask64, bcs64, True, c64["dx"], 0.5, 1, "SSPRK2")
+    t0 = time.perf_counter()
+    CO.run_roe_exner(st64, mask64, bcs64, True, c64["dx"], 0.5, steps64, "SSPRK2")
+    v64 = n * n * steps64 / (time.perf_counter() - t0)
+    cores = _cores()
+    sample = (f"{n}x{n} Gaussian-bed case (the workload itself), {args.warmup} + {args.steps} SSPRK2 steps, "
+              f"float32 C/OpenMP restatement of the reference step, {cores} threads")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded Gaussian bed)",
-            "config": {"workload": "roe_exner_gaussian_bed_2048x2048_mpm_ssprk2 (512x512 CPU sample)"},
+            "config": {"workload": f"roe_exner_gaussian_bed_{n}x{n}_mpm_ssprk2_f32", "cells": n * n},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "fp64_port": {"value": v64, "unit": UNIT, "steps": steps64, "cores": cores,
+                          "sample": f"{n}x{n}, {steps64} SSPRK2 steps, float64 build (the oracle)"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def oracle_reference_run(n, steps, path):
+    """Float64 C/OpenMP oracle on the Gaussian-bed case at n x n for ``steps`` SSPRK2
+    steps, final state to ``path`` (.npz).  Run in a spawned process beside the GPU work."""
+    from oracle import c_oracle as CO
+
+    c, bcs, st, mask = _oracle_case(n, np.float64)
+    t0 = time.perf_counter()
+    out, _ = CO.run_roe_exner(st, mask, bcs, True, c["dx"], 0.5, steps, "SSPRK2")
+    np.savez(path, sec=time.perf_counter() - t0, **{k: out[k] for k in ("h", "hu", "hv", "z", "z_b")})
+
+
+def errors_vs(a, ref):
+    """rel-L1 and Linf (relative to max |ref|) of h, hu, hv and the total bed z + z_b over
+    the physical cells."""
+    s = (slice(1, -1), slice(1, -1))
+    out = {}
+    for name, x, y in (("h", a["h"], ref["h"]), ("hu", a["hu"], ref["hu"]), ("hv", a["hv"], ref["hv"]),
+                       ("bed", a["z"] + a["z_b"], ref["z"] + ref["z_b"])):
+        x, y = np.asarray(x, np.float64)[s], np.asarray(y, np.float64)[s]
+        out[name] = {"rel_l1": float(np.sum(np.abs(x - y)) / max(np.sum(np.abs(y)), 1e-300)),
+                     "linf": float(np.max(np.abs(x - y)) / max(np.max(np.abs(y)), 1e-300))}
+    return out
 
 
 def profile_sequence(args):
@@ -514,6 +597,8 @@ def main():
     ap.add_argument("--n", type=int, default=2048)
     ap.add_argument("--impl", default="b200")
     ap.add_argument("--accuracy-steps", type=int, default=2000)
+    ap.add_argument("--oracle-n", type=int, default=1024,
+                    help="side of the accuracy case run by the float64 C oracle as well (0 to skip)")
     ap.add_argument("--n-big", type=int, default=8192, help="side of the bandwidth case (0 to skip)")
     ap.add_argument("--big-steps", type=int, default=20)
     ap.add_argument("--transport-u", type=float, default=1.0,
@@ -613,18 +698,32 @@ def main():
     # ---- end to end through the public API with host buffers
     e2e_sec, h2d, d2h = e2e_run(n, torch.float32, args.steps, args.warmup)
     e2e_val = ncell * args.steps / e2e_sec
-    acc = accuracy_run(n, args.accuracy_steps) if args.accuracy_steps > 0 else None
-    ens = ensemble_run(args.ensemble_members, args.ensemble_steps) if args.ensemble_members > 0 else None
+    # ---- CPU baseline (rank 0): the reference step's C restatement on the workload, while
+    # the GPU is idle
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        v, cores, sample = cpu_oracle_sample(n, 10.0)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+    # ---- accuracy: the float64 oracle runs in a spawned process while the GPU works
+    oracle_proc, oracle_path = None, None
+    if rank == 0 and args.accuracy_steps > 0 and args.oracle_n > 0 and not args.no_cpu:
+        import multiprocessing as mp
+        import tempfile
+
+        oracle_path = os.path.join(tempfile.mkdtemp(prefix="pxb_oracle_"), "ref.npz")
+        oracle_proc = mp.get_context("spawn").Process(target=oracle_reference_run,
+                                                      args=(args.oracle_n, args.accuracy_steps, oracle_path))
+        oracle_proc.start()
+    ens = (ensemble_run(args.ensemble_members, args.ensemble_steps, world=world, rank=rank)
+           if args.ensemble_members > 0 else None)
     roe = plain_roe_run() if rank == 0 and not args.no_cpu else None
+    acc = (accuracy_run(n, args.accuracy_steps, args.oracle_n, oracle_proc, oracle_path)
+           if args.accuracy_steps > 0 else None)
     if rank != 0:
         if world > 1:
             dist.barrier()
             dist.destroy_process_group()
         return
-    cpu = None
-    if not args.no_cpu:
-        v, cores, sample = cpu_oracle_sample(512, 10.0)
-        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps, "higher_is_better": True,

@@ -183,6 +183,30 @@ int pxb_re_stage(pxb_re_plan* plan, const pxb_re_fields* in, const pxb_re_fields
 int pxb_re_run(pxb_re_plan* plan, const pxb_re_fields* a, const pxb_re_fields* b, int32_t nsteps,
                int32_t scheme, double cfl, double t0, void* dt_log, void* stream);
 
+/* Water and sediment volume budget.  The reference advances every cell by flux
+ * differences (the fluctuation scatter and update of roe_exner.py:597-606, the Exner
+ * update of roe_exner.py:708-715), so over the physical cells (rows and columns 1 .. n-2
+ * that are not nodata) the interior faces telescope: the volumes change by the flux
+ * through their outer boundary, up to rounding.
+ *
+ * pxb_re_volume: volumes[0] = sum h dx^2, volumes[1] = sum z_b dx^2 over the physical
+ * cells (host array of 2), summed in float64 with Neumaier compensation in a fixed order.
+ * Allocates a small scratch on its first call; synchronises `stream`.
+ *
+ * pxb_re_set_budget: acc_dev (device array of 4 doubles, zeroed by the caller) receives,
+ * during every later pxb_re_run, the water and sediment volume that left the physical
+ * cells through their boundary faces: acc[0] + acc[1] (water, m^3), acc[2] + acc[3]
+ * (sediment, m^3), each pair a Neumaier sum and its compensation, accumulated in float64.
+ * The face flux is the one the fluctuations telescope to: for a face with left (west or
+ * north) cell I, h_I u_n,I + upwM_0 for water and the upwind Exner flux for sediment;
+ * each stage adds dt dx times its boundary sum, times 1/2 under SSPRK2.  Then
+ * volume(end) - volume(start) + outflow vanishes to rounding.  Fused stage path only
+ * (PXB_ERR_UNSUPPORTED otherwise); acc_dev = NULL switches it off.  The first call with
+ * an accumulator allocates the per-item partial array (16 bytes per work item of the
+ * shortest band geometry). */
+int pxb_re_volume(pxb_re_plan* plan, const pxb_re_fields* f, double* volumes, void* stream);
+int pxb_re_set_budget(pxb_re_plan* plan, double* acc_dev);
+
 /* Tangent-linear model (forward-mode derivative) of pxb_re_init / pxb_re_run, float64
  * plans only.  No counterpart in the reference's code (JAX would give it with jax.jvp).
  * The state planes and their tangents (every plane of both structs set) advance together:
@@ -218,6 +242,30 @@ int pxb_re_jvp_run(pxb_re_plan* plan, const pxb_re_fields* a, const pxb_re_field
 int pxb_re_vjp_init(pxb_re_plan* plan, const pxb_re_fields* f, const pxb_re_fields* fbar, void* stream);
 int pxb_re_vjp_run(pxb_re_plan* plan, const pxb_re_fields* a0, int32_t nsteps, int32_t scheme, double cfl, double t0,
                    int32_t checkpoint_every, const pxb_re_fields* abar, void* stream);
+
+/* Adjoints of the scalar parameters, the reverse-mode counterparts of
+ * pxb_re_tangent_params (host arrays, ADDED to; either may be NULL):
+ *   seds_bar[7 * nsed]   dJ/d(sediment matrix) of pnetcdf_reader.py:136-158 (row 1: the
+ *                        grain diameter d50) through the MPM grass factor (roe_exner.py:85-130)
+ *                        of every stage and the init, and through n_b = n_p_mix of compute_n
+ *                        (roe_exner.py:64-73) in the friction of every Roe face; one sediment
+ *                        class (PXB_ERR_UNSUPPORTED otherwise);
+ *   values0_bar[nh]      dJ/d(values[0]) of each ConstantInflux handler (plan order), the
+ *                        discharge of roeexner_constantinflux.py:29-30 (0 for other kinds).
+ * pxb_re_vjp_run_params: as pxb_re_vjp_run; with seds_bar set, abar->n_b (when not NULL;
+ * in: dJ/dn_b of the final state, n_b being constant) receives dJ/dn_b of a0.
+ * pxb_re_vjp_init_params: as pxb_re_vjp_init; with seds_bar set, fbar->n_b (in: dJ/dn_b
+ * after init) goes through compute_n to fbar->n (when set) and to the matrix, and leaves
+ * zero.  The parameter sums use atomics, so their last bits can vary between runs. */
+typedef struct pxb_re_param_adjoints {
+    double* seds_bar;
+    double* values0_bar;
+} pxb_re_param_adjoints;
+int pxb_re_vjp_init_params(pxb_re_plan* plan, const pxb_re_fields* f, const pxb_re_fields* fbar,
+                           const pxb_re_param_adjoints* pbar, void* stream);
+int pxb_re_vjp_run_params(pxb_re_plan* plan, const pxb_re_fields* a0, int32_t nsteps, int32_t scheme, double cfl,
+                          double t0, int32_t checkpoint_every, const pxb_re_fields* abar,
+                          const pxb_re_param_adjoints* pbar, void* stream);
 
 /* Device error word of the plan (non-finite dt or state seen by a kernel): reads it
  * (synchronising `stream`), clears it, returns PXB_OK or PXB_ERR_NONFINITE. */
@@ -294,17 +342,17 @@ int pxb_re_ens_check(pxb_re_ens* ens, void* stream, int32_t* first_bad);
 /* No counterpart in the reference: PyExner's JAX step never manages device memory
  * itself.  For callers that cannot allocate device memory when they need dt -- an XLA
  * custom call, which must work inside the buffers XLA has already allocated; a host
- * application whose policy forbids cudaMalloc after start-up; code recording a stream
- * capture, which an allocation would break.  Same result as pxb_re_cfl, without a plan:
- * dt = max(cfl * min over active faces of dx / speed, 1e-6), written to dt_dev (one
- * element of dtype).  nodata may be NULL.  Calls no cudaMalloc/cudaFree: the reduction
- * scratch is a fixed array of (8192 + 32) * 8 bytes in device memory owned by the
- * library, resident on every device that loads it until the process exits.  Grids up
- * to 31 * 8192 = 253952 columns wide (any height); wider grids return PXB_ERR_ARG.
- * The first call on a device looks up the array's device address; make that first call
- * before any stream capture.  All calls share the array: calls whose kernels can
- * overlap on the GPU (unordered streams, or several host threads on one device) race
- * and must be serialised by the caller. */
+ * application whose policy forbids cudaMalloc after start-up.  Same result as
+ * pxb_re_cfl, without a plan: dt = max(cfl * min over active faces of dx / speed, 1e-6),
+ * written to dt_dev (one element of dtype).  nodata may be NULL.  Calls no
+ * cudaMalloc/cudaFree: the reduction scratch is a fixed array of (8192 + 32) * 8 bytes in
+ * device memory owned by the library, resident on every device that loads it until the
+ * process exits.  Grids up to 31 * 8192 = 253952 columns wide (any height); wider grids
+ * return PXB_ERR_ARG.  The first call on a device (and the first after cudaDeviceReset)
+ * looks up the array's device address; make that first call before any stream capture.
+ * All calls share the array: calls whose kernels can overlap on the GPU (unordered
+ * streams, or several host threads on one device) race and must be serialised by the
+ * caller. */
 int pxb_re_cfl_noalloc(int32_t ny, int32_t nx, int64_t pitch, int32_t dtype, double dx, double cfl,
                        const void* h, const void* hu, const void* hv, const void* G, const uint8_t* nodata,
                        void* dt_dev, void* stream);

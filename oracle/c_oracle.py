@@ -36,27 +36,35 @@ class _State(ctypes.Structure):
     _fields_ = [(n, ctypes.c_void_p) for n in ("h", "hu", "hv", "z", "zb", "n", "nb", "G")]
 
 
+OUT32 = os.path.join(HERE, "c", "build", "libre_oracle_f32.so")
+
+
 def build(force=False):
-    if not force and os.path.exists(OUT) and os.path.getmtime(OUT) >= os.path.getmtime(SRC):
-        return OUT
+    """Both builds of the restatement: float64 (the oracle) and float32 (the same
+    operations on a float32 state, as the reference runs as shipped)."""
     os.makedirs(os.path.dirname(OUT), exist_ok=True)
-    subprocess.run(["gcc", "-O2", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared", SRC,
-                    "-o", OUT, "-lm"], check=True)
+    for out, real in ((OUT, "double"), (OUT32, "float")):
+        if not force and os.path.exists(out) and os.path.getmtime(out) >= os.path.getmtime(SRC):
+            continue
+        subprocess.run(["gcc", "-O2", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared",
+                        f"-DOC_REAL={real}", SRC, "-o", out, "-lm"], check=True)
     return OUT
 
 
-_lib = None
+_libs = {}
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        _lib = ctypes.CDLL(build())
-        _lib.oc_re_run.argtypes = [ctypes.POINTER(_Case), ctypes.POINTER(_State), ctypes.c_int, ctypes.c_int,
-                                   ctypes.c_double, ctypes.c_void_p]
-        _lib.oc_re_run.restype = ctypes.c_int
-        _lib.oc_re_init.argtypes = [ctypes.POINTER(_Case), ctypes.POINTER(_State)]
-    return _lib
+def lib(dtype=np.float64):
+    key = np.dtype(dtype).name
+    if key not in _libs:
+        build()
+        L = ctypes.CDLL(OUT if key == "float64" else OUT32)
+        L.oc_re_run.argtypes = [ctypes.POINTER(_Case), ctypes.POINTER(_State), ctypes.c_int, ctypes.c_int,
+                                ctypes.c_double, ctypes.c_void_p]
+        L.oc_re_run.restype = ctypes.c_int
+        L.oc_re_init.argtypes = [ctypes.POINTER(_Case), ctypes.POINTER(_State)]
+        _libs[key] = L
+    return _libs[key]
 
 
 def _case(shape, bcs, mask0, mpm, seds, dx, keep):
@@ -88,31 +96,32 @@ def _case(shape, bcs, mask0, mpm, seds, dx, keep):
     return c
 
 
-def _state(st, keep):
-    arrs = {k: np.ascontiguousarray(np.array(st[k], dtype=np.float64)) for k in
+def _state(st, keep, dtype=np.float64):
+    arrs = {k: np.ascontiguousarray(np.array(st[k], dtype=dtype)) for k in
             ("h", "hu", "hv", "z", "z_b", "n", "n_b", "G")}
     keep.append(arrs)
     s = _State(*[arrs[k].ctypes.data for k in ("h", "hu", "hv", "z", "z_b", "n", "n_b", "G")])
     return s, arrs
 
 
-def init(st, mask, bcs, mpm, dx=1.0):
+def init(st, mask, bcs, mpm, dx=1.0, dtype=np.float64):
     keep = []
     c = _case(st["h"].shape, bcs, mask[0], mpm, st["seds"], dx, keep)
-    s, arrs = _state(st, keep)
-    lib().oc_re_init(ctypes.byref(c), ctypes.byref(s))
+    s, arrs = _state(st, keep, dtype)
+    lib(dtype).oc_re_init(ctypes.byref(c), ctypes.byref(s))
     out = dict(arrs)
     out["seds"] = st["seds"]
     return out
 
 
-def run_roe_exner(st, mask, bcs, mpm, dx, cfl, nsteps, scheme):
-    """Same contract as oracle.integrators.run_roe_exner (st must already be initialised)."""
+def run_roe_exner(st, mask, bcs, mpm, dx, cfl, nsteps, scheme, dtype=np.float64):
+    """Same contract as oracle.integrators.run_roe_exner (st must already be initialised);
+    dtype np.float32 runs the float32 build on a float32 copy of the state."""
     keep = []
     c = _case(st["h"].shape, bcs, mask[0], mpm, st["seds"], dx, keep)
-    s, arrs = _state(st, keep)
+    s, arrs = _state(st, keep, dtype)
     dts = np.zeros(max(1, nsteps))
-    rc = lib().oc_re_run(ctypes.byref(c), ctypes.byref(s), int(nsteps), 1 if scheme == "SSPRK2" else 0, float(cfl),
+    rc = lib(dtype).oc_re_run(ctypes.byref(c), ctypes.byref(s), int(nsteps), 1 if scheme == "SSPRK2" else 0, float(cfl),
                          dts.ctypes.data)
     if rc != 0:
         raise MemoryError("C oracle: allocation failed")

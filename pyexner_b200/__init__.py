@@ -11,14 +11,20 @@ from .integrators import (
     IntegratorBundle,
     IntegratorConfig,
     create_integrator_bundle,
+    new_budget,
+    outflow,
     register_integrator_bundle,
     run_steps,
+    volume,
 )
 from .solvers import SOLVER_REGISTRY, SolverBundle, SolverConfig, create_solver_bundle, register_solver_bundle
 from .state import STATE_REGISTRY, RoeExnerState, RoeState, create_state, register_state
 
 __all__ = [
     "run_driver",
+    "new_budget",
+    "outflow",
+    "volume",
     "BoundaryManager",
     "RoeState",
     "RoeExnerState",

@@ -47,6 +47,10 @@ class BcHandler(ctypes.Structure):
     ]
 
 
+class ParamAdjoints(ctypes.Structure):
+    _fields_ = [("seds_bar", c_void_p), ("values0_bar", c_void_p)]
+
+
 class REFields(ctypes.Structure):
     _fields_ = [(n, c_void_p) for n in ("h", "hu", "hv", "z", "z_b", "n", "n_b", "G")]
 
@@ -159,6 +163,11 @@ SIGNATURES = {
     "pxb_label_polygons": [c_int32, c_int32, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p, c_void_p,
                            c_int64, c_void_p],
     "pxb_version": [],
+    "pxb_re_volume": [c_void_p, POINTER(REFields), POINTER(c_double), c_void_p],
+    "pxb_re_vjp_run_params": [c_void_p, POINTER(REFields), c_int32, c_int32, c_double, c_double, c_int32,
+                              POINTER(REFields), c_void_p, c_void_p],
+    "pxb_re_vjp_init_params": [c_void_p, POINTER(REFields), POINTER(REFields), c_void_p, c_void_p],
+    "pxb_re_set_budget": [c_void_p, c_void_p],
 }
 
 

@@ -30,6 +30,7 @@ UNITS = [
     ("kernels_adj.cu", ["-fmad=false"]),
     ("capi.cu", []),
     ("noalloc.cu", []),
+    ("noalloc_f64.cu", ["-fmad=false"]),
 ]
 
 

@@ -114,11 +114,54 @@ __global__ void __launch_bounds__(256) adj_exner_kernel(const AdjArgs a) {
     adj_dt_add(a.dtbar, add_dt);
 }
 
-// grass factor backwards, in place on T (G of the state after handlers 1 -> h, hu, hv)
-__global__ void adj_grass_kernel(const AdjArgs a) {
+// warp sum of each of N values, one atomic per value and warp (every lane calls this)
+template <int N>
+__device__ __forceinline__ void adj_sum_add(double* dst, const double (&v)[N]) {
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+        double x = v[q];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(FULL, x, o);
+        if ((threadIdx.x & 31) == 0 && x != 0.0) atomicAdd(dst + q, x);
+    }
+}
+
+// grass factor backwards, in place on T (G of the state after handlers 1 -> h, hu, hv);
+// PAR: also the adjoint of the MPM constants of the single sediment class (a.tbar), from
+// one evaluation on dual numbers seeded in the cell's h, hu, hv and in those constants
+template <bool PAR>
+__global__ void __launch_bounds__(256) adj_grass_kernel(const AdjArgs a) {
     int r, c;
     long long i;
-    if (!adj_cell(a.ny, a.nx, a.pitch, r, c, i)) return;
+    const bool in = adj_cell(a.ny, a.nx, a.pitch, r, c, i);
+    if constexpr (PAR) {
+        double tb[7] = {0, 0, 0, 0, 0, 0, 0};
+        if (in && a.mpm) {
+            using D = DualN<10>;
+            const bool m = adj_nodata(a.nodata, i);
+            SedTable<D> sd;
+            sd.n = 1;
+            sd.s[0].np2 = D::seed(a.sed.s[0].np2, 3);
+            sd.s[0].sm1d = D::seed(a.sed.s[0].sm1d, 4);
+            sd.s[0].thc = D::seed(a.sed.s[0].thc, 5);
+            sd.s[0].np3sg = D::seed(a.sed.s[0].np3sg, 6);
+            sd.s[0].sm1 = D::seed(a.sed.s[0].sm1, 7);
+            sd.s[0].frac = D::seed(a.sed.s[0].frac, 8);
+            sd.one_minus_por = D::seed(a.sed.one_minus_por, 9);
+            const D G = mpm_grass(D::seed(a.sh[i], 0), D::seed(a.shu[i], 1), D::seed(a.shv[i], 2), m, sd);
+            const double gbar = a.TG[i];
+            a.Th[i] += gbar * G.d[0];
+            a.Thu[i] += gbar * G.d[1];
+            a.Thv[i] += gbar * G.d[2];
+            a.TG[i] = 0.0;
+#pragma unroll
+            for (int q = 0; q < 7; ++q) tb[q] = gbar * G.d[3 + q];
+        } else if (in) {
+            a.TG[i] = (!adj_nodata(a.nodata, i) && a.sh[i] > DRY_TOL) ? a.TG[i] : 0.0;
+        }
+        adj_sum_add<7>(a.tbar, tb);
+        return;
+    }
+    if (!in) return;
     const bool m = adj_nodata(a.nodata, i);
     const double gbar = a.TG[i];
     if (a.mpm) {
@@ -162,23 +205,25 @@ __global__ void adj_corr_kernel(const AdjArgs a) {
     if (!(active && !stop_v)) a.Thv[i] = 0.0;
 }
 
-// hydro update backwards: I += T (identity paths) + face terms; dt adjoint
+// hydro update backwards: I += T (identity paths) + face terms; dt adjoint.  NB: a fifth
+// tangent in the cell's n_b (Manning friction of its faces) adds its adjoint to a.nbbar.
+template <bool NB>
 __global__ void __launch_bounds__(256) adj_hydro_kernel(const AdjArgs a) {
     int r, c;
     long long i;
     const bool in = adj_cell(a.ny, a.nx, a.pitch, r, c, i);
     double add_dt = 0.0;
     if (in) {
-        using D = DualN<4>;
+        using D = DualN<NB ? 5 : 4>;
         const double dt = *a.dt, dx = a.dx, DRY = DRY_TOL;
         const HCell<D> Cd = make_hcell(D::seed(a.h[i], 0), D::seed(a.hu[i], 1), D::seed(a.hv[i], 2),
-                                       D::seed(a.zb[i], 3), D(a.z[i]), D(a.nb[i]));
+                                       D::seed(a.zb[i], 3), D(a.z[i]), NB ? D::seed(a.nb[i], NB ? 4 : 0) : D(a.nb[i]));
         auto hconst = [&](long long k) {
             return make_hcell(D(a.h[k]), D(a.hu[k]), D(a.hv[k]), D(a.zb[k]), D(a.z[k]), D(a.nb[k]));
         };
         const bool mC = adj_nodata(a.nodata, i);
         const double k_ = -dt / dx;
-        double g[4] = {0, 0, 0, 0};
+        double g[NB ? 5 : 4] = {};
         double f[3] = {0, 0, 0};  // forward fluctuation sum of this cell
         // face (I|J): M goes to I, P to J
         auto face = [&](long long k, bool cell_is_I, bool yf) {
@@ -195,7 +240,7 @@ __global__ void __launch_bounds__(256) adj_hydro_kernel(const AdjArgs a) {
             }
             const long long I = cell_is_I ? i : k, J = cell_is_I ? k : i;
             const double aI[3] = {a.Th[I], a.Thu[I], a.Thv[I]}, aJ[3] = {a.Th[J], a.Thu[J], a.Thv[J]};
-            for (int q = 0; q < 4; ++q)
+            for (int q = 0; q < (NB ? 5 : 4); ++q)
                 for (int m = 0; m < 3; ++m) g[q] += k_ * (aI[m] * M[m].d[q] + aJ[m] * P[m].d[q]);
             for (int m = 0; m < 3; ++m) f[m] += cell_is_I ? M[m].v : P[m].v;
         };
@@ -208,6 +253,7 @@ __global__ void __launch_bounds__(256) adj_hydro_kernel(const AdjArgs a) {
         a.Ihv[i] += a.Thv[i] + g[2];
         a.Izb[i] += a.Tzb[i] + g[3];
         a.IG[i] += a.TG[i];
+        if constexpr (NB) a.nbbar[i] += g[NB ? 4 : 0];
         add_dt = -(a.Th[i] * f[0] + a.Thu[i] * f[1] + a.Thv[i] * f[2]) / dx;
     }
     adj_dt_add(a.dtbar, add_dt);
@@ -275,9 +321,35 @@ __global__ void adj_bc_scatter_kernel(const AdjBcArgs a) {
             if (a.c0 != a.c0) add(1, t[1 * n + k]);
             if (a.c1 != a.c1) add(2, t[2 * n + k]);
             break;
-        default:  // ConstantInflux, Berthon: prescribed values
+        case PXB_BC_RE_CONSTANTINFLUX:  // prescribed hu = q values[1], hv = q values[2]: the adjoint of q
+            if (a.qbar) {
+                const double v = t[1 * n + k] * a.vx + t[2 * n + k] * a.vy;
+                if (v != 0.0) atomicAdd(a.qbar, v);
+            }
+            break;
+        default:  // Berthon: prescribed values
             break;
     }
+}
+
+// compute_n of the initialisation backwards (roe_exner.py:64-73): n_b = n_p_mix where the
+// raw z_b > SED_TOL (MPM), the raw n elsewhere (and everywhere with a constant grass
+// factor).  The n_b adjoint moves to n (when nbar is set) or to n_p_mix (summed into
+// *npbar); n_b's own value before the initialisation has no influence.
+__global__ void __launch_bounds__(256) adj_compute_n_kernel(int ny, int nx, long long pitch, int mpm,
+                                                            const double* zb, double* nbbar, double* nbar,
+                                                            double* npbar) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.y * blockDim.y + threadIdx.y;
+    double v[1] = {0.0};
+    if (r < ny && c < nx) {
+        const long long i = (long long)r * pitch + c;
+        const double b = nbbar[i];
+        if (mpm && zb[i] > SED_TOL) v[0] = b;
+        else if (nbar) nbar[i] += b;
+        nbbar[i] = 0.0;
+    }
+    adj_sum_add<1>(npbar, v);
 }
 
 // ---------------------------------------------------------------- dt backwards

@@ -21,6 +21,9 @@ struct AdjArgs {
     double *Th, *Thu, *Thv, *Tzb, *TG;  // adjoint of the state entering the Exner update
     double *Ih, *Ihu, *Ihv, *Izb, *IG;  // adjoint of the stage input (accumulated)
     double* dtbar;                      // accumulated adjoint of dt
+    // parameter adjoints (null: not requested)
+    double* nbbar;  // plane: adjoint of the static n_b (friction of the Roe faces), accumulated
+    double* tbar;   // MPM table of the one sediment class: np2, sm1d, thc, np3sg, sm1, frac, 1 - porosity
 };
 
 // Field slots as BcArgs: 0 h, 1 hu, 2 hv, 3 z_b, 4 n (not carried), 5 G.
@@ -32,6 +35,8 @@ struct AdjBcArgs {
     double nx, ny;
     double c0, c1;  // ZeroMomentum values (NaN: identity)
     double* tmp;    // 6 * count
+    double vx, vy;  // ConstantInflux: d(hu, hv) / d values[0] = (values[1], values[2])
+    double* qbar;   // ConstantInflux: adjoint of its values[0] (accumulated; null: not requested)
 };
 
 struct AdjCflArgs {

@@ -635,6 +635,12 @@ struct pxb_re_plan {
     int want_rows = 0;
     pxb::SedTable<float> sedf;
     pxb::SedTable<double> sedd;
+    // volume budget (pxb_re_set_budget / pxb_re_volume): per-item outflow partials of the
+    // stage kernel, the caller's accumulator, and the volume reduction's scratch
+    double* bud_part = nullptr;
+    long long bud_items = 0;
+    pxb::BudgetAcc* bud_acc = nullptr;
+    double* vol_scr = nullptr;
 };
 
 struct pxb_roe_plan {
@@ -759,7 +765,7 @@ int re_cfl_impl(pxb_re_plan* P, const pxb_re_fields* f, double cfl, void* dt_out
 
 template <class T>
 int re_stage_impl(pxb_re_plan* P, const pxb_re_fields* in, const pxb_re_fields* out, const pxb_re_fields* avg,
-                  const void* dt, cudaStream_t s) {
+                  const void* dt, cudaStream_t s, double bud_w = 0.0) {
     pxb::REStageArgs<T> a{};
     a.ny = P->c.ny;
     a.nx = P->c.nx;
@@ -795,7 +801,12 @@ int re_stage_impl(pxb_re_plan* P, const pxb_re_fields* in, const pxb_re_fields* 
     a.nbands = g.nbands;
     a.err = &P->c.scr->err;
     a.queue = P->c.scr->queue;
+    const long long nitems = (long long)pxb_stage_items_per_band(g.nstrips) * g.nbands;
+    const bool bud = bud_w > 0.0 && P->bud_acc && P->bud_part && nitems <= P->bud_items;
+    if (bud) a.bud = P->bud_part;
     PXB_CUDA(pxb::launch_re_stage<T>(a, P->mpm != 0, P->nodata != nullptr, avg != nullptr, g.grid, s));
+    if (bud)
+        PXB_CUDA(pxb::launch_budget_stage<T>(P->bud_part, (int)nitems, (const T*)dt, bud_w * P->c.dx, P->bud_acc, s));
     return PXB_OK;
 }
 
@@ -987,12 +998,13 @@ int re_autotune_impl(pxb_re_plan* P, const pxb_re_fields* A, const pxb_re_fields
 
 // One stage on the plan's path; the general path reads the time from *tptr or tval.
 int re_stage_any(pxb_re_plan* P, const pxb_re_fields* in, const pxb_re_fields* out, const pxb_re_fields* avg,
-                 const void* dt, const double* tptr, double tval, cudaStream_t s) {
+                 const void* dt, const double* tptr, double tval, cudaStream_t s, double bud_w = 0.0) {
     const bool f64 = P->c.dtype == PXB_F64;
     if (P->path == PXB_PATH_GENERAL)
         return f64 ? re_general_impl<double>(P, in, out, avg, dt, tptr, tval, s)
                    : re_general_impl<float>(P, in, out, avg, dt, tptr, tval, s);
-    return f64 ? re_stage_impl<double>(P, in, out, avg, dt, s) : re_stage_impl<float>(P, in, out, avg, dt, s);
+    return f64 ? re_stage_impl<double>(P, in, out, avg, dt, s, bud_w)
+               : re_stage_impl<float>(P, in, out, avg, dt, s, bud_w);
 }
 
 int re_steps(pxb_re_plan* P, const pxb_re_fields* A, const pxb_re_fields* B, int nsteps, int scheme, double cfl,
@@ -1005,8 +1017,11 @@ int re_steps(pxb_re_plan* P, const pxb_re_fields* A, const pxb_re_fields* B, int
     };
     // the time of the step is the one the CFL launch before the stage recorded
     const double* tdev = &P->c.scr->t_step;
+    // with a budget accumulator set, every stage adds its boundary outflow weighted by the
+    // integrator: u^{n+1} - u^n = -dt R(u^n) (Forward Euler), -dt/2 (R(u^n) + R(u^(1))) (SSPRK2)
+    const double bud_w = (P->bud_acc && !general) ? (scheme == PXB_SSPRK2 ? 0.5 : 1.0) : 0.0;
     auto stage_call = [&](const pxb_re_fields* in, const pxb_re_fields* out, const pxb_re_fields* avg,
-                          cudaStream_t st) { return re_stage_any(P, in, out, avg, P->c.dt_dev, tdev, 0.0, st); };
+                          cudaStream_t st) { return re_stage_any(P, in, out, avg, P->c.dt_dev, tdev, 0.0, st, bud_w); };
     // static planes of b are those of a; the general path carries n in b as well
     pxb_re_fields Bs = *B;
     Bs.z = A->z;
@@ -1021,6 +1036,7 @@ int re_steps(pxb_re_plan* P, const pxb_re_fields* A, const pxb_re_fields* B, int
     std::vector<const void*> key = {A->h, A->hu, A->hv, A->z_b, A->G, A->z, A->n_b, A->n, B->h, B->hu, B->hv,
                                     B->z_b, B->G, Bs.n, dt_log, (const void*)(intptr_t)scheme};
     key.push_back(*(const void* const*)&cfl_d);
+    key.push_back((const void*)P->bud_acc);
     PXB_CUDA(cudaMemsetAsync(&P->c.scr->step, 0, sizeof(unsigned int), s));
     // only the general path has handlers that read the time
     if (general)
@@ -1550,11 +1566,16 @@ int zero5(PlanCommon& C, const Planes5& q, cudaStream_t s) {
     return PXB_OK;
 }
 
-// Handlers backwards (last to first) on adjoint planes (slots h, hu, hv, z_b, -, G).
-int adj_handlers(PlanCommon& C, double* const f[6], double* tmp, cudaStream_t s) {
+// Handlers backwards (last to first) on adjoint planes (slots h, hu, hv, z_b, -, G);
+// qbar (device, one per handler, or null) accumulates the adjoints of the ConstantInflux
+// discharges values[0].
+int adj_handlers(PlanCommon& C, double* const f[6], double* tmp, cudaStream_t s, double* qbar = nullptr) {
     for (size_t q = C.handlers.size(); q-- > 0;) {
         const DevHandler& h = C.handlers[q];
         pxb::AdjBcArgs b{};
+        b.vx = h.vx;
+        b.vy = h.vy;
+        b.qbar = qbar ? qbar + q : nullptr;
         for (int k = 0; k < 6; ++k) b.f[k] = f[k];
         b.cells = h.cells;
         b.donors = h.donors;
@@ -1581,6 +1602,11 @@ struct AdjWork {
     unsigned long long* maxbits = nullptr;
     unsigned int* nties = nullptr;
     double* bctmp = nullptr;
+    // parameter adjoints (null: not requested): per handler the ConstantInflux discharge,
+    // then the MPM table of the sediment class; the n_b adjoint plane
+    double* qbar = nullptr;
+    double* tbar = nullptr;
+    double* nbbar = nullptr;
     Planes5 ck(int k) const { return planes_of(base, plane, k); }                  // checkpoint k
     Planes5 seg(int k) const { return planes_of(base, plane, nck + k); }           // segment state k
     void release() {
@@ -1672,13 +1698,15 @@ int adj_stage(pxb_re_plan* P, AdjWork& W, const pxb_re_fields* in, const Planes5
     a.Izb = aIn.p[3];
     a.IG = aIn.p[4];
     a.dtbar = W.dev + 1;
+    a.nbbar = W.nbbar;
+    a.tbar = W.tbar;
     double* const fS[6] = {W.aS.p[0], W.aS.p[1], W.aS.p[2], W.aS.p[3], nullptr, W.aS.p[4]};
-    st = adj_handlers(P->c, fS, W.bctmp, s);  // handlers 2
+    st = adj_handlers(P->c, fS, W.bctmp, s, W.qbar);  // handlers 2
     if (st != PXB_OK) return st;
     PXB_CUDA(pxb::launch_adj_stage(a, 0, s));  // Exner
     PXB_CUDA(pxb::launch_adj_stage(a, 1, s));  // grass
     double* const fT[6] = {W.aT.p[0], W.aT.p[1], W.aT.p[2], W.aT.p[3], nullptr, W.aT.p[4]};
-    st = adj_handlers(P->c, fT, W.bctmp, s);  // handlers 1
+    st = adj_handlers(P->c, fT, W.bctmp, s, W.qbar);  // handlers 1
     if (st != PXB_OK) return st;
     PXB_CUDA(pxb::launch_adj_stage(a, 2, s));  // corrections
     PXB_CUDA(pxb::launch_adj_stage(a, 3, s));  // hydro
@@ -1704,12 +1732,64 @@ int adj_step_fwd(pxb_re_plan* P, AdjWork& W, const Planes5& u, const Planes5& ne
     return copy5(P->c, next, W.u1, s);
 }
 
+// Device array of the parameter adjoints of one reverse-mode call: nh handler discharges,
+// then the 7 MPM table entries of the sediment class and the adjoint of n_p_mix.
+int param_adjoint_buffer(pxb_re_plan* P, const pxb_re_param_adjoints* pa, double** out) {
+    *out = nullptr;
+    if (!pa || (!pa->seds_bar && !pa->values0_bar)) return PXB_OK;
+    if (pa->seds_bar && P->mpm && P->nsed != 1)
+        return fail(PXB_ERR_UNSUPPORTED, "sediment-matrix adjoints are built for one sediment class");
+    const size_t n = P->c.handlers.size() + 8;
+    PXB_CUDA(cudaMalloc(out, sizeof(double) * n));
+    PXB_CUDA(cudaMemset(*out, 0, sizeof(double) * n));
+    return PXB_OK;
+}
+
+// The accumulated parameter adjoints into the caller's host arrays: discharges directly;
+// the MPM table (and n_p_mix) to the sediment matrix through the derivatives of the
+// table with respect to each matrix entry (fill_sed_dual, the tangent model's table).
+int apply_param_adjoints(pxb_re_plan* P, const double* dev, const pxb_re_param_adjoints* pa, cudaStream_t s) {
+    if (!dev) return PXB_OK;
+    const size_t nh = P->c.handlers.size();
+    std::vector<double> h(nh + 8);
+    PXB_CUDA(cudaMemcpyAsync(h.data(), dev, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s));
+    PXB_CUDA(cudaStreamSynchronize(s));
+    if (pa->values0_bar)
+        for (size_t k = 0; k < nh; ++k)
+            if (P->c.handlers[k].kind == PXB_BC_RE_CONSTANTINFLUX) pa->values0_bar[k] += h[k];
+    if (pa->seds_bar && P->mpm) {
+        const double* tb = h.data() + nh;  // np2, sm1d, thc, np3sg, sm1, frac, 1 - porosity, n_p_mix
+        const int ns = P->nsed;
+        std::vector<double> unit(7 * (size_t)ns, 0.0);
+        for (int e = 0; e < 7 * ns; ++e) {
+            unit[e] = 1.0;
+            pxb::SedTable<pxb::Dual> S;
+            fill_sed_dual(S, P->seds.data(), unit.data(), ns);
+            unit[e] = 0.0;
+            const pxb::SedT<pxb::Dual>& c = S.s[0];
+            pa->seds_bar[e] += tb[0] * c.np2.d + tb[1] * c.sm1d.d + tb[2] * c.thc.d + tb[3] * c.np3sg.d +
+                               tb[4] * c.sm1.d + tb[5] * c.frac.d + tb[6] * S.one_minus_por.d + tb[7] * S.n_p_mix.d;
+        }
+    }
+    return PXB_OK;
+}
+
 int vjp_run_impl(pxb_re_plan* P, const pxb_re_fields* a0, int nsteps, int scheme, double cfl, double t0, int every,
-                 const pxb_re_fields* abar, cudaStream_t s) {
+                 const pxb_re_fields* abar, const pxb_re_param_adjoints* pa, cudaStream_t s) {
     for (auto& h : P->c.handlers)
         if (h.kind == PXB_BC_RE_CONSTANTOUTFLUX)
             return fail(PXB_ERR_UNSUPPORTED, "the reverse mode does not cover ConstantOutflux handlers (nonlinear)");
+    double* pdev = nullptr;
+    {
+        const int pst = param_adjoint_buffer(P, pa, &pdev);
+        if (pst != PXB_OK) return pst;
+    }
     AdjWork W;
+    if (pdev) {
+        W.qbar = pdev;
+        if (pa->seds_bar && P->mpm) W.tbar = pdev + P->c.handlers.size();
+        if (pa->seds_bar && abar->n_b) W.nbbar = (double*)abar->n_b;
+    }
     W.K = every > 0 ? every : 32;
     W.nck = (nsteps + W.K - 1) / W.K;
     W.plane = (size_t)P->c.ny * (size_t)P->c.pitch;
@@ -1720,6 +1800,7 @@ int vjp_run_impl(pxb_re_plan* P, const pxb_re_fields* a0, int nsteps, int scheme
     auto bail = [&](int code) {
         cudaStreamSynchronize(s);
         W.release();
+        cudaFree(pdev);
         return code;
     };
     if (cudaMalloc(&W.base, sizeof(double) * nplanes * W.plane) != cudaSuccess ||
@@ -1849,23 +1930,34 @@ int vjp_run_impl(pxb_re_plan* P, const pxb_re_fields* a0, int nsteps, int scheme
         }
     }
     if (st == PXB_OK) chk(copy5(P->c, AB, W.aNext, s));
+    if (st == PXB_OK) chk(apply_param_adjoints(P, pdev, pa, s));
     cudaStreamSynchronize(s);
     W.release();
+    cudaFree(pdev);
     return st;
 }
 
 // init_fn_roeexner backwards: handlers (t = 0), then the grass factor from the raw state.
-int vjp_init_impl(pxb_re_plan* P, const pxb_re_fields* f, const pxb_re_fields* fbar, cudaStream_t s) {
+int vjp_init_impl(pxb_re_plan* P, const pxb_re_fields* f, const pxb_re_fields* fbar, const pxb_re_param_adjoints* pa,
+                  cudaStream_t s) {
     for (auto& h : P->c.handlers)
         if (h.kind == PXB_BC_RE_CONSTANTOUTFLUX)
             return fail(PXB_ERR_UNSUPPORTED, "the reverse mode does not cover ConstantOutflux handlers (nonlinear)");
+    double* pdev = nullptr;
+    {
+        const int pst = param_adjoint_buffer(P, pa, &pdev);
+        if (pst != PXB_OK) return pst;
+    }
     int maxcount = 1;
     for (auto& h : P->c.handlers) maxcount = std::max(maxcount, h.count);
     double* tmp = nullptr;
-    PXB_CUDA(cudaMalloc(&tmp, sizeof(double) * 6 * (size_t)maxcount));
+    if (cudaMalloc(&tmp, sizeof(double) * 6 * (size_t)maxcount) != cudaSuccess) {
+        cudaFree(pdev);
+        return fail(PXB_ERR_CUDA, "reverse-mode handler buffer");
+    }
     double* const fb[6] = {(double*)fbar->h, (double*)fbar->hu, (double*)fbar->hv, (double*)fbar->z_b, nullptr,
                            (double*)fbar->G};
-    int st = adj_handlers(P->c, fb, tmp, s);
+    int st = adj_handlers(P->c, fb, tmp, s, pdev);
     if (st == PXB_OK) {
         pxb::AdjArgs a{};
         a.ny = P->c.ny;
@@ -1882,10 +1974,18 @@ int vjp_init_impl(pxb_re_plan* P, const pxb_re_fields* f, const pxb_re_fields* f
         a.Thu = fb[1];
         a.Thv = fb[2];
         a.TG = fb[5];
+        if (pdev && pa->seds_bar && P->mpm) a.tbar = pdev + P->c.handlers.size();
         if (pxb::launch_adj_stage(a, 1, s) != cudaSuccess) st = fail(PXB_ERR_CUDA, "adjoint of the grass factor");
     }
+    // compute_n: the n_b adjoint to the raw n and to n_p_mix (the sediment matrix)
+    if (st == PXB_OK && pdev && pa->seds_bar && fbar->n_b &&
+        pxb::launch_adj_compute_n(P->c.ny, P->c.nx, P->c.pitch, P->mpm, (const double*)f->z_b, (double*)fbar->n_b,
+                                  (double*)fbar->n, pdev + P->c.handlers.size() + 7, s) != cudaSuccess)
+        st = fail(PXB_ERR_CUDA, "adjoint of compute_n");
+    if (st == PXB_OK) st = apply_param_adjoints(P, pdev, pa, s);
     cudaStreamSynchronize(s);
     cudaFree(tmp);
+    cudaFree(pdev);
     return st;
 }
 
@@ -2014,6 +2114,8 @@ int pxb_re_plan_destroy(pxb_re_plan* plan) {
     cudaFree(plan->jvp);
     cudaFree(plan->dscr);
     cudaFree(plan->jvp_tmp);
+    cudaFree(plan->bud_part);
+    cudaFree(plan->vol_scr);
     delete plan;
     return PXB_OK;
 }
@@ -2087,6 +2189,43 @@ int pxb_re_run(pxb_re_plan* P, const pxb_re_fields* a, const pxb_re_fields* b, i
     return re_steps(P, a, b, nsteps, scheme, cfl, t0, dt_log, (cudaStream_t)stream);
 }
 
+int pxb_re_set_budget(pxb_re_plan* P, double* acc_dev) {
+    if (!P) return fail(PXB_ERR_ARG, "null plan");
+    if (acc_dev && P->path != PXB_PATH_FUSED)
+        return fail(PXB_ERR_UNSUPPORTED, "the volume budget is built into the fused stage path only");
+    if (acc_dev && ((uintptr_t)acc_dev & 7u)) return fail(PXB_ERR_ARG, "acc_dev must be 8-byte aligned");
+    if (acc_dev && !P->bud_part) {
+        // every band height the plan can take (the autotuner goes down to 8 rows)
+        const int nstrips = std::max(1, (P->c.nx - 3 + pxb_stage_strip_out((int)P->c.esize()) - 1) /
+                                            pxb_stage_strip_out((int)P->c.esize()));
+        const long long items = (long long)pxb_stage_items_per_band(nstrips) * ((P->c.ny - 1 + 7) / 8 + 1);
+        PXB_CUDA(cudaMalloc(&P->bud_part, sizeof(double) * 2 * (size_t)items));
+        P->bud_items = items;
+    }
+    P->bud_acc = (pxb::BudgetAcc*)acc_dev;
+    return PXB_OK;
+}
+
+int pxb_re_volume(pxb_re_plan* P, const pxb_re_fields* f, double* volumes, void* stream) {
+    if (!P) return fail(PXB_ERR_ARG, "null plan");
+    if (!f || !f->h || !f->z_b) return fail(PXB_ERR_ARG, "h and z_b must be set");
+    if (!volumes) return fail(PXB_ERR_ARG, "volumes is null");
+    const int nblocks = std::max(1, std::min(P->c.ny - 2, 4 * P->c.sm_count));
+    if (!P->vol_scr) PXB_CUDA(cudaMalloc(&P->vol_scr, sizeof(double) * (4 * (size_t)(4 * P->c.sm_count) + 2)));
+    cudaStream_t s = (cudaStream_t)stream;
+    double* out = P->vol_scr + 4 * (size_t)(4 * P->c.sm_count);
+    const double dx2 = P->c.dx * P->c.dx;
+    if (P->c.dtype == PXB_F64)
+        PXB_CUDA(pxb::launch_volume<double>(P->c.ny, P->c.nx, P->c.pitch, (const double*)f->h, (const double*)f->z_b,
+                                            P->nodata, P->vol_scr, nblocks, dx2, out, s));
+    else
+        PXB_CUDA(pxb::launch_volume<float>(P->c.ny, P->c.nx, P->c.pitch, (const float*)f->h, (const float*)f->z_b,
+                                           P->nodata, P->vol_scr, nblocks, dx2, out, s));
+    PXB_CUDA(cudaMemcpyAsync(volumes, out, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    PXB_CUDA(cudaStreamSynchronize(s));
+    return PXB_OK;
+}
+
 int pxb_re_jvp_init(pxb_re_plan* P, const pxb_re_fields* f, const pxb_re_fields* f_dot,
                     const pxb_re_tangent_params* tp, void* stream) {
     if (!P) return fail(PXB_ERR_ARG, "null plan");
@@ -2118,17 +2257,29 @@ int pxb_re_jvp_run(pxb_re_plan* P, const pxb_re_fields* a, const pxb_re_fields* 
     return st;
 }
 
-int pxb_re_vjp_init(pxb_re_plan* P, const pxb_re_fields* f, const pxb_re_fields* fbar, void* stream) {
+int pxb_re_vjp_init_params(pxb_re_plan* P, const pxb_re_fields* f, const pxb_re_fields* fbar,
+                           const pxb_re_param_adjoints* pbar, void* stream) {
     if (!P) return fail(PXB_ERR_ARG, "null plan");
     if (P->c.dtype != PXB_F64) return fail(PXB_ERR_ARG, "the reverse mode runs on float64 plans");
     if (!f || !f->h || !f->hu || !f->hv) return fail(PXB_ERR_ARG, "state: h, hu and hv must be set");
     if (!fbar || !fbar->h || !fbar->hu || !fbar->hv || !fbar->z_b || !fbar->G)
         return fail(PXB_ERR_ARG, "adjoint: h, hu, hv, z_b and G must be set");
-    return vjp_init_impl(P, f, fbar, (cudaStream_t)stream);
+    if (pbar && pbar->seds_bar && fbar->n_b && !f->z_b) return fail(PXB_ERR_ARG, "state: z_b must be set");
+    return vjp_init_impl(P, f, fbar, pbar, (cudaStream_t)stream);
+}
+
+int pxb_re_vjp_init(pxb_re_plan* P, const pxb_re_fields* f, const pxb_re_fields* fbar, void* stream) {
+    return pxb_re_vjp_init_params(P, f, fbar, nullptr, stream);
 }
 
 int pxb_re_vjp_run(pxb_re_plan* P, const pxb_re_fields* a0, int32_t nsteps, int32_t scheme, double cfl, double t0,
                    int32_t checkpoint_every, const pxb_re_fields* abar, void* stream) {
+    return pxb_re_vjp_run_params(P, a0, nsteps, scheme, cfl, t0, checkpoint_every, abar, nullptr, stream);
+}
+
+int pxb_re_vjp_run_params(pxb_re_plan* P, const pxb_re_fields* a0, int32_t nsteps, int32_t scheme, double cfl,
+                          double t0, int32_t checkpoint_every, const pxb_re_fields* abar,
+                          const pxb_re_param_adjoints* pbar, void* stream) {
     if (!P) return fail(PXB_ERR_ARG, "null plan");
     if (P->c.dtype != PXB_F64) return fail(PXB_ERR_ARG, "the reverse mode runs on float64 plans");
     if (!a0 || !a0->h || !a0->hu || !a0->hv || !a0->z || !a0->z_b || !a0->n_b || !a0->G)
@@ -2138,7 +2289,7 @@ int pxb_re_vjp_run(pxb_re_plan* P, const pxb_re_fields* a0, int32_t nsteps, int3
     if (nsteps < 0) return fail(PXB_ERR_ARG, "nsteps < 0");
     if (scheme != PXB_FE && scheme != PXB_SSPRK2) return fail(PXB_ERR_ARG, "scheme must be PXB_FE or PXB_SSPRK2");
     if (nsteps == 0) return PXB_OK;
-    return vjp_run_impl(P, a0, nsteps, scheme, cfl, t0, checkpoint_every, abar, (cudaStream_t)stream);
+    return vjp_run_impl(P, a0, nsteps, scheme, cfl, t0, checkpoint_every, abar, pbar, (cudaStream_t)stream);
 }
 
 int pxb_re_check(pxb_re_plan* P, void* stream) {

@@ -20,10 +20,22 @@ cudaError_t launch_adj_stage(const AdjArgs& a, int phase, cudaStream_t s) {
     const dim3 g = adj_grid(a.ny, a.nx), b(32, 8);
     switch (phase) {
         case 0: adj_exner_kernel<<<g, b, 0, s>>>(a); break;
-        case 1: adj_grass_kernel<<<g, b, 0, s>>>(a); break;
+        case 1:
+            if (a.tbar) adj_grass_kernel<true><<<g, b, 0, s>>>(a);
+            else adj_grass_kernel<false><<<g, b, 0, s>>>(a);
+            break;
         case 2: adj_corr_kernel<<<g, b, 0, s>>>(a); break;
-        default: adj_hydro_kernel<<<g, b, 0, s>>>(a); break;
+        default:
+            if (a.nbbar) adj_hydro_kernel<true><<<g, b, 0, s>>>(a);
+            else adj_hydro_kernel<false><<<g, b, 0, s>>>(a);
+            break;
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adj_compute_n(int ny, int nx, long long pitch, int mpm, const double* zb, double* nbbar,
+                                 double* nbar, double* npbar, cudaStream_t s) {
+    adj_compute_n_kernel<<<adj_grid(ny, nx), dim3(32, 8), 0, s>>>(ny, nx, pitch, mpm, zb, nbbar, nbar, npbar);
     return cudaGetLastError();
 }
 

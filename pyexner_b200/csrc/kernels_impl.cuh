@@ -6,7 +6,9 @@ namespace pxb {
 
 template <class T, bool MPM, bool HM, bool AVG>
 static cudaError_t stage_variant(const REStageArgs<T>& a, int grid, cudaStream_t s) {
-    re_stage_kernel<T, MPM, HM, AVG><<<grid, 128, 0, s>>>(a);
+    // the budget variant only when its partial array is set (the others carry no budget code)
+    if (a.bud) re_stage_kernel<T, MPM, HM, AVG, true><<<grid, 128, 0, s>>>(a);
+    else re_stage_kernel<T, MPM, HM, AVG, false><<<grid, 128, 0, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -160,6 +162,23 @@ cudaError_t launch_roe_stage(const RoeArgs<T>& a, bool avg, cudaStream_t s) {
 }
 
 template <class T>
+cudaError_t launch_budget_stage(const double* part, int nitems, const T* dt, double w_dx, BudgetAcc* acc,
+                                cudaStream_t s) {
+    budget_stage_kernel<T><<<1, 256, 0, s>>>(part, nitems, dt, w_dx, acc);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t launch_volume(int ny, int nx, long long pitch, const T* h, const T* zb, const uint8_t* nodata,
+                          double* part, int nblocks, double dx2, double* out, cudaStream_t s) {
+    volume_kernel<T><<<nblocks, 256, 0, s>>>(ny, nx, pitch, h, zb, nodata, part);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    volume_final_kernel<<<1, 32, 0, s>>>(part, nblocks, dx2, out);
+    return cudaGetLastError();
+}
+
+template <class T>
 cudaError_t launch_roe_cfl(const CflArgs<T>& a, int grid, cudaStream_t s) {
     roe_cfl_kernel<T><<<grid, 256, 0, s>>>(a);
     return cudaGetLastError();
@@ -178,6 +197,9 @@ cudaError_t launch_roe_cfl(const CflArgs<T>& a, int grid, cudaStream_t s) {
     template cudaError_t launch_ens_cfl<T>(const EnsCflArgs<T>&, bool, int, cudaStream_t);              \
     template cudaError_t launch_set_time<T>(CflScratch*, double, cudaStream_t);                         \
     template cudaError_t launch_roe_stage<T>(const RoeArgs<T>&, bool, cudaStream_t);                    \
-    template cudaError_t launch_roe_cfl<T>(const CflArgs<T>&, int, cudaStream_t);
+    template cudaError_t launch_roe_cfl<T>(const CflArgs<T>&, int, cudaStream_t);                      \
+    template cudaError_t launch_budget_stage<T>(const double*, int, const T*, double, BudgetAcc*, cudaStream_t); \
+    template cudaError_t launch_volume<T>(int, int, long long, const T*, const T*, const uint8_t*, double*, int, \
+                                          double, double*, cudaStream_t);
 
 }  // namespace pxb

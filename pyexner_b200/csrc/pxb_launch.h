@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "budget.cuh"
 #include "ens.cuh"
 #include "init_bc.cuh"
 #include "re_cfl.cuh"
@@ -32,6 +33,14 @@ template <class T>
 cudaError_t launch_re_cfl(const CflArgs<T>& a, bool has_mask, int grid, cudaStream_t s);
 template <class T>
 int re_cfl_blocks_per_sm(bool has_mask);
+// Volume budget (budget.cuh): one stage's boundary outflow into the accumulator; the
+// water and bed volumes of a state into out[2] (device).
+template <class T>
+cudaError_t launch_budget_stage(const double* part, int nitems, const T* dt, double w_dx, BudgetAcc* acc,
+                                cudaStream_t s);
+template <class T>
+cudaError_t launch_volume(int ny, int nx, long long pitch, const T* h, const T* zb, const uint8_t* nodata,
+                          double* part, int nblocks, double dx2, double* out, cudaStream_t s);
 template <class T>
 cudaError_t launch_re_init(const InitArgs<T>& a, cudaStream_t s);
 template <class T>
@@ -52,6 +61,8 @@ cudaError_t launch_adj_store(int ny, int nx, long long pitch, double scale, cons
 cudaError_t launch_adj_stage(const AdjArgs& a, int phase, cudaStream_t s);
 cudaError_t launch_adj_bc(const AdjBcArgs& a, cudaStream_t s);
 cudaError_t launch_adj_cfl(const AdjCflArgs& a, cudaStream_t s);
+cudaError_t launch_adj_compute_n(int ny, int nx, long long pitch, int mpm, const double* zb, double* nbbar,
+                                 double* nbar, double* npbar, cudaStream_t s);
 
 // Tangent-linear model (kernels_dual.cu).
 cudaError_t launch_dual_cfl(const DualCflArgs& a, cudaStream_t s);

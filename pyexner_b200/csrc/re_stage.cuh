@@ -73,6 +73,11 @@ struct REStageArgs {
     int band_rows, nstrips, nbands;
     int* err;
     unsigned int* queue;  // {next dynamic item, finished blocks}, zero between launches
+    // Volume budget (null: off): per work item, the outflow through the outer boundary of
+    // the physical cells (rows and columns 1 .. n-2) of water (sum of the mass fluxes of
+    // the boundary faces) and of sediment (Exner fluxes), in the state's flux units; item
+    // k writes bud[2k], bud[2k+1] on every launch.
+    double* bud;
 };
 
 // Asynchronous global -> shared copies of one element (cp.async, completion by group).
@@ -87,6 +92,11 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// cp.async of 16 bytes with zero fill: the first src_bytes (0-16) bytes are read, the
+// rest of the 16 is set to zero; with src_bytes = 0 nothing is read.
+__device__ __forceinline__ void cp_async16_zfill(unsigned smem, const void* gmem, unsigned src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem), "l"(gmem), "r"(src_bytes) : "memory");
+}
 static_assert(sizeof(pxb_ring_recipe) == 48, "ring recipes are copied as three 16-byte chunks");
 
 // Fields of the second boundary application (z_b and G donors) packed into one word by
@@ -191,7 +201,7 @@ __device__ __forceinline__ void read_cols(const T* rowp, int lane, T (&v)[CPT]) 
 // consecutive columns (pxb_stage_cpt): a strip is 32 * CPT columns, 3 halo | owned | 3
 // halo.  Neighbour values inside a lane are plain registers; across lanes one shuffle
 // moves the first (east) or last (west) column.
-template <class T, bool MPM, bool HAS_MASK, bool AVG>
+template <class T, bool MPM, bool HAS_MASK, bool AVG, bool BUD = false>
 __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int item, bool& bad) {
     constexpr int CPT = pxb_stage_cpt((int)sizeof(T));
     constexpr int W = 32 * CPT;
@@ -230,6 +240,20 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
         // boundary recipes can only apply in the first/last strip or on rows 0 / ny-1
         const bool bc_strip = (a.ring != nullptr) && (strip == 0 || last_strip);
         const bool bc_rows = (a.ring != nullptr) && (R0 == 0 || R1 == ny);
+        // Budget: only items that own boundary faces of physical cells add to the lane slots.
+        // A face counts once: in the item that owns its row (x-faces; y-faces (r-1|r) by row
+        // r) and, for columns, by the lane that owns the column.  The outflow of a face with
+        // left cell I (west / north side) is F = h_I u_n,I + upwM_0, the flux whose
+        // differences the fluctuations of roe_exner.py:597-606 telescope to; F leaves the
+        // physical cells through the east / south boundary and enters them through the west
+        // / north one.  Exner: the upwind face flux of roe_exner.py:708-715.
+        // (BUD: the budget instantiation, launched only when a.bud is set)
+        __shared__ double budbuf[4][BUD ? 2 : 1][BUD ? 32 : 1];
+        const bool bud_item = BUD && (bc_strip || bc_rows);
+        if constexpr (BUD) {
+            budbuf[threadIdx.x >> 5][0][lane] = 0.0;
+            budbuf[threadIdx.x >> 5][1][lane] = 0.0;
+        }
 
         // ---- carried pipeline state, per column
         HCell<T> pA[CPT];
@@ -462,6 +486,11 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
                         P[k][m] = xact[k] ? P[k][m] : T(0);
                         M[k][m] = xact[k] ? M[k][m] : T(0);
                     }
+                    if (bud_item && xact[k] && out_col[k] && r >= R0 && r < R1 && r >= 1 && r <= ny - 2 &&
+                        (cb + k == 0 || cb + k == nx - 2)) {
+                        const double F = (double)mul_rn(pr[k].h, pr[k].u) + (double)M[k][0];
+                        if constexpr (BUD) budbuf[threadIdx.x >> 5][0][lane] += cb + k == 0 ? -F : F;
+                    }
                 }
                 // upwP of the west face of column k: own column k-1, or the west lane's last
                 // (lane 0 has no west face in the warp).  P and M are zero on inactive faces,
@@ -499,6 +528,14 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
                     for (int m = 0; m < 3; ++m) {
                         yP[k][m] = yact ? yP[k][m] : T(0);
                         yM[k][m] = yact ? yM[k][m] : T(0);
+                    }
+                    if (bud_item && (r == 1 || r == ny - 1) && r >= R0 && r < R1) {
+                        const int c = cb + k;
+                        if (out_col[k] && yact && c >= 1 && c <= nx - 2) {
+                            // y-faces have the normal (0, -1): u_n = -v
+                            const double F = -(double)mul_rn(pA[k].h, pA[k].v) + (double)yM[k][0];
+                            if constexpr (BUD) budbuf[threadIdx.x >> 5][0][lane] += r == 1 ? -F : F;
+                        }
                     }
                 }
             }
@@ -713,6 +750,9 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
                         xact[k] = rowD && has_e[k] && exner_active(e3[k], ee[k], mq[k], mqe[k]);
                         const T Fx = exner_face<T, false>(e3[k], ee[k]);
                         F[k] = xact[k] ? Fx : T(0);
+                        if (bud_item && xact[k] && out_col[k] && q >= R0 && q < R1 && q >= 1 && q <= ny - 2 &&
+                            (cb + k == 0 || cb + k == nx - 2))
+                            if constexpr (BUD) budbuf[threadIdx.x >> 5][1][lane] += cb + k == 0 ? -(double)F[k] : (double)F[k];
                     }
                     T Fw[CPT];
                     bool wact[CPT];
@@ -728,6 +768,9 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
                         const bool yex = rowD && (S || q - 1 >= L0) && colok[k] && exner_active(e4[k], e3[k], mq1[k], mq[k]);
                         const T Fyv = exner_face<T, true>(e4[k], e3[k]);
                         Fy[k] = yex ? Fyv : T(0);
+                        if (bud_item && yex && out_col[k] && (q == 1 || q == ny - 1) && q >= R0 && q < R1 &&
+                            cb + k >= 1 && cb + k <= nx - 2)
+                            if constexpr (BUD) budbuf[threadIdx.x >> 5][1][lane] += q == 1 ? -(double)Fy[k] : (double)Fy[k];
                     }
                 }
             }
@@ -859,6 +902,18 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
         // later iterations would only advance the halo rows below the band
         for (; r < R1 + 5; ++r) iterate(r, std::false_type{});
         cp_async_wait<0>();  // the buffers are reused by the next item
+        if constexpr (BUD) {  // this item's outflow: the warp's slots in a fixed order
+            double bh = budbuf[threadIdx.x >> 5][0][lane], bz = budbuf[threadIdx.x >> 5][1][lane];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                bh += __shfl_down_sync(FULL, bh, o);
+                bz += __shfl_down_sync(FULL, bz, o);
+            }
+            if (lane == 0) {
+                a.bud[2 * item] = bh;
+                a.bud[2 * item + 1] = bz;
+            }
+        }
     }
 }
 
@@ -866,7 +921,7 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
 // warp index; further items come from a grid-wide queue (one atomic per item), so warps
 // on lightly loaded SMs take more of them and no SM waits on a fixed share.  The last
 // block to finish resets the queue for the next launch on the stream.
-template <class T, bool MPM, bool HAS_MASK, bool AVG>
+template <class T, bool MPM, bool HAS_MASK, bool AVG, bool BUD = false>
 __global__ void __launch_bounds__(128, PXB_STAGE_BOUNDS(T, AVG)) re_stage_kernel(const REStageArgs<T> a) {
     const int lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -874,7 +929,7 @@ __global__ void __launch_bounds__(128, PXB_STAGE_BOUNDS(T, AVG)) re_stage_kernel
     bool bad = false;
     int item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     while (item < nitems) {
-        re_stage_item<T, MPM, HAS_MASK, AVG>(a, item, bad);
+        re_stage_item<T, MPM, HAS_MASK, AVG, BUD>(a, item, bad);
         unsigned next = 0;
         if (lane == 0) next = atomicAdd(&a.queue[0], 1u);
         item = nw + (int)__shfl_sync(FULL, next, 0);

@@ -28,6 +28,23 @@ from .solvers import _dtype_code, _stream
 from .state import alloc_plane
 
 
+def partition_members(cells, world):
+    """Split ensemble members over ``world`` ranks (one process per GPU, replicas only:
+    no data crosses ranks).  ``cells``: the cell count of every member.  Returns one
+    sorted list of member indices per rank: members are dealt largest first to the rank
+    with the fewest cells so far (ties to the lower rank), so every rank computes the same
+    split on its own and the ranks finish close together."""
+    if world < 1:
+        raise ValueError("world must be at least 1")
+    load = [0] * world
+    parts = [[] for _ in range(world)]
+    for k in sorted(range(len(cells)), key=lambda i: (-int(cells[i]), i)):
+        r = min(range(world), key=lambda j: (load[j], j))
+        parts[r].append(k)
+        load[r] += int(cells[k])
+    return [sorted(p) for p in parts]
+
+
 class Ensemble:
     def __init__(self, members, erosion, dtype=None, band_rows=0):
         if not members:

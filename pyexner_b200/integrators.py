@@ -74,25 +74,61 @@ def scratch_like(state):
     return type(state)(**kw)
 
 
-def run_steps(state, mask, solver_config, scheme, n_steps, cfl, scratch=None, log_dt=True, t0=0.0):
+def run_steps(state, mask, solver_config, scheme, n_steps, cfl, scratch=None, log_dt=True, t0=0.0, budget=None):
     """Advance ``state`` IN PLACE by ``n_steps`` steps on the device, starting at time
     ``t0`` (the step times are accumulated on the device).
 
     Returns the device tensor of the dts taken (or None).  ``scratch`` is a second
-    state of the same layout (allocated when not given)."""
+    state of the same layout (allocated when not given).  ``budget`` (Roe-Exner, fused
+    stage path): a float64 device tensor from ``new_budget`` into which every step adds
+    the water and sediment volume that left the physical cells through their boundary
+    (read it with ``outflow``)."""
     code = _lib.SSPRK2 if scheme == "SSPRK2" else _lib.FE
     b = scratch if scratch is not None else scratch_like(state)
     dts = torch.empty(max(1, n_steps), dtype=state.dtype, device=state.h.device) if log_dt else None
     dptr = ctypes.c_void_p(dts.data_ptr()) if dts is not None else None
     if isinstance(state, RoeExnerState):
         plan = _re_plan(state, mask, solver_config)
-        _lib.call("pxb_re_run", plan.handle, ctypes.byref(state.c_fields()), ctypes.byref(b.c_fields()),
-                  int(n_steps), code, float(cfl), float(t0), dptr, _stream())
+        if budget is not None:
+            if budget.dtype != torch.float64 or budget.numel() != 4 or budget.device != state.h.device:
+                raise ValueError("budget must be the float64 device tensor of new_budget()")
+            _lib.call("pxb_re_set_budget", plan.handle, ctypes.c_void_p(budget.data_ptr()))
+        try:
+            _lib.call("pxb_re_run", plan.handle, ctypes.byref(state.c_fields()), ctypes.byref(b.c_fields()),
+                      int(n_steps), code, float(cfl), float(t0), dptr, _stream())
+        finally:
+            if budget is not None:
+                _lib.call("pxb_re_set_budget", plan.handle, None)
     else:
+        if budget is not None:
+            raise ValueError("the volume budget is kept for Roe-Exner states")
         plan = _roe_plan(state, solver_config)
         _lib.call("pxb_roe_run", plan.handle, ctypes.byref(state.c_fields()), ctypes.byref(b.c_fields()),
                   int(n_steps), code, float(cfl), dptr, _stream())
     return dts[:n_steps] if dts is not None else None
+
+
+def new_budget(device="cuda"):
+    """A zeroed boundary-outflow accumulator for ``run_steps(..., budget=...)``: float64
+    water and sediment outflow volumes (m^3), each with its compensation term."""
+    return torch.zeros(4, dtype=torch.float64, device=device)
+
+
+def outflow(budget):
+    """(water, sediment) volumes (m^3) that left the physical cells, from ``budget``."""
+    b = budget.detach().cpu().numpy()
+    return float(b[0] + b[1]), float(b[2] + b[3])
+
+
+def volume(state, mask, solver_config):
+    """(water, erodible bed) volume in m^3 of the physical cells of a Roe-Exner state:
+    sum h dx^2 and sum z_b dx^2 over rows and columns 1 .. n-2 that are not nodata,
+    compensated float64 sums in a fixed order.  Together with the outflow of
+    ``run_steps(..., budget=...)``, volume(end) - volume(start) + outflow is rounding."""
+    plan = _re_plan(state, mask, solver_config)
+    out = (ctypes.c_double * 2)()
+    _lib.call("pxb_re_volume", plan.handle, ctypes.byref(state.c_fields()), out, _stream())
+    return float(out[0]), float(out[1])
 
 
 def autotune(state, mask, solver_config, scratch=None):

@@ -4,8 +4,9 @@ For a state ``u`` and a direction ``u_dot`` (a second RoeExnerState holding the 
 of every plane), ``jvp_run`` advances both through ``n_steps`` integrator steps: the
 values exactly as ``run_steps`` does in float64, the tangents by the chain rule through
 every stage, including the dependence of dt on the state (through the fastest face).
-This is what ``jax.jvp`` of the reference's loop would give; gradients of a scalar
-objective follow one direction at a time (a full adjoint is not provided).
+This is what ``jax.jvp`` of the reference's loop would give.  The reverse mode
+(``vjp_run`` / ``vjp_init``, further down) gives the gradient of a scalar objective with
+respect to every plane of the initial state in one backward sweep.
 
 ``RoeExnerSteps`` wraps the run as a ``torch.autograd.Function`` with a forward-mode
 rule, so ``torch.autograd.forward_ad`` dual tensors flow through it.

@@ -2,7 +2,7 @@
 
 Run (in the container that holds the reference checkout; not on the GPU box):
 
-    python tests/golden/make_golden.py /root/reference/src/PyExner
+    python tests/golden/make_golden.py <checkout>/src/PyExner
 
 It imports PyExner's modules from that source tree with ``jaxshim`` standing in for
 ``jax.numpy`` (float64 numpy, i.e. the reference's math with x64 enabled) and stubs
@@ -393,7 +393,9 @@ def run_roe_cases(mods):
 
 
 def main():
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src/PyExner"
+    if len(sys.argv) < 2:
+        raise SystemExit("usage: make_golden.py <path to the reference's src/PyExner>")
+    src = sys.argv[1]
     mods = load_reference(src)
     np.seterr(all="ignore")
     run_face_kernels(mods)

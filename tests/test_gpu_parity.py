@@ -88,8 +88,11 @@ def test_roe_exner_golden(request, case, dtype):
     ((37, 30), 6, "smooth", "trans_x_refl_y", True),
     ((66, 58), 11, "fast", "refl_self", True),
 ])
-def test_roe_exner_strips_and_bands(shape, band_rows, regime, bc, mpm):
-    """Grids spanning several warp strips and row bands, checked against the oracle."""
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "f32"])
+def test_roe_exner_strips_and_bands(shape, band_rows, regime, bc, mpm, dtype):
+    """Grids spanning several warp strips and row bands, checked against the oracle: in
+    float64 the fused kernel's register pipeline, in float32 its shared-memory row
+    pipeline (26 owned columns per strip, so every layout here crosses strip edges)."""
     from pyexner_b200 import run_steps
     from pyexner_b200.cases import seds_matrix
 
@@ -102,14 +105,31 @@ def test_roe_exner_strips_and_bands(shape, band_rows, regime, bc, mpm):
     odt = ORE.compute_dt(ost, 0.5, dx, omask[0])
     o1 = ORE.stage(ost, odt, dx, omask, obcs, mpm)
     orun, odts = OI.run_roe_exner(ost, omask, obcs, mpm, dx, 0.5, 4, "SSPRK2")
-    bundle, cfg, mask, st = device_re(arrs, params, X, Y, seds, torch.float64, dx)
-    assert_planes(st.to_numpy(), ost, 1e-12, what="init")
+    tol1, tolN = TOL[dtype]
+    g_tol = 2e-4 if dtype == torch.float32 else None
+    if dtype == torch.float32 and regime == "wetdry":
+        # Ill-conditioned in float32: a dry cell next to fast wet cells takes a depth of a
+        # few 1e-4 m as the difference of O(0.1) fluxes (relative rounding ~3e-5) and a
+        # velocity of up to ~200 m/s, which the bedload (~u^3 ~ h^-3) and the next steps
+        # amplify.  The general path, a separate cell-parallel kernel chain, shows the same
+        # errors; the comparison with it below holds the strip decomposition to rounding.
+        tol1, tolN = 2e-4, 5e-3
+    bundle, cfg, mask, st = device_re(arrs, params, X, Y, seds, dtype, dx)
+    assert_planes(st.to_numpy(), ost, tol1, what="init", g_tol=g_tol)
     s1 = bundle.step_fn(st, 0.0, float(odt), mask, cfg)
-    assert_planes(s1.to_numpy(), o1, 1e-12, what="stage")
+    assert_planes(s1.to_numpy(), o1, tol1, what="stage", g_tol=g_tol)
     s = st.clone()
     dts = run_steps(s, mask, cfg, "SSPRK2", 4, 0.5)
-    assert rel_err(dts.cpu().numpy(), odts) <= 1e-10
-    assert_planes(s.to_numpy(), orun, 1e-10, what="ssprk2")
+    assert rel_err(dts.cpu().numpy(), odts) <= tolN
+    assert_planes(s.to_numpy(), orun, tolN, what="ssprk2")
+    if dtype == torch.float32:
+        gparams = dict(params, stage_path="general")
+        gb, gcfg, gmask, gst = device_re(arrs, gparams, X, Y, seds, dtype, dx)
+        g1 = gb.step_fn(gst, 0.0, float(odt), gmask, gcfg)
+        assert_planes(g1.to_numpy(), s1.to_numpy(), 1e-6, what="fused vs general stage")
+        gs = gst.clone()
+        run_steps(gs, gmask, gcfg, "SSPRK2", 4, 0.5)
+        assert_planes(gs.to_numpy(), s.to_numpy(), 1e-6, what="fused vs general ssprk2")
 
 
 def test_ssprk2_stage_api_matches_run_loop():

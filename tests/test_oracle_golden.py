@@ -133,3 +133,22 @@ def test_c_oracle_matches_golden(request, case):
         assert np.max(np.abs(dts - d[f"{tag}_dts"])) <= 1e-15
         for k in RE.STATE_FIELDS:
             close(out[k], d[f"{tag}_{k}"], 1e-13, 1e-300)
+
+
+@pytest.mark.parametrize("case", CASES[:3], ids=[c[0] for c in CASES[:3]])
+def test_c_oracle_float32_build_tracks_golden(request, case):
+    """The float32 build of the C restatement (the reference's own precision, timed by
+    bench.py's reference arm) stays within float32 rounding of the float64 golden run."""
+    from oracle import c_oracle as CO
+
+    d, bcs, mask, st, mpm = load_re_case(request.config.rootpath, case)
+    if any(hd.kind not in CO.KINDS for hd in bcs.handlers):
+        pytest.skip("the C restatement carries the four boundary types of the benchmark layouts only")
+    st = CO.init(st, mask, bcs, mpm, 0.1, dtype=np.float32)
+    assert st["h"].dtype == np.float32
+    out, dts = CO.run_roe_exner(st, mask, bcs, mpm, 0.1, 0.5, NSTEPS, "SSPRK2", dtype=np.float32)
+    assert np.max(np.abs(dts - d["rk_dts"])) <= 1e-4 * np.max(np.abs(d["rk_dts"]))
+    for k in ("h", "hu", "hv", "z_b"):
+        ref = d[f"rk_{k}"]
+        ok = ~np.isnan(ref)
+        assert np.max(np.abs(out[k][ok] - ref[ok])) <= 1e-4 * max(1e-3, np.max(np.abs(ref[ok]))), k
