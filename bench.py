@@ -419,6 +419,51 @@ def ensemble_run(count, steps, seed=0, world=1, rank=0):
             "dt_range": [float(d.min()), float(d.max())], "l2": "state ~1.1 GB, larger than L2"}
 
 
+def adjoint_run(n=512, steps=64, every=32):
+    """Configuration 4's reverse mode (float64): ``steps`` SSPRK2 steps of the 512 x 512
+    inflow case forward, then the checkpointed backward sweep with the parameter adjoints
+    (discharge, sediment matrix); device time per step of each."""
+    import torch
+
+    from pyexner_b200 import BoundaryManager, RoeExnerState, cases, create_solver_bundle, run_steps
+    from pyexner_b200.tangent import ParamAdjoints, vjp_init, vjp_run
+
+    arrs, params, X, Y, target = cases.adjoint_case(n)
+    bm = BoundaryManager(params, X, Y)
+    raw = RoeExnerState.from_numpy(arrs, cases.seds_matrix(params["erosion"]), torch.float64)
+    bundle = create_solver_bundle("Roe Exner")
+    cfg = bundle.config(raw, None, bm, 0.01, params)
+    mask = bundle.mask_fn(raw, None, bm.boundary_mask)
+    st0 = bundle.init_fn(raw, mask, cfg)
+    st = st0.clone()
+    run_steps(st.clone(), mask, cfg, "SSPRK2", 2, 0.5, log_dt=False)  # graph capture
+    torch.cuda.synchronize()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    e[0].record()
+    run_steps(st, mask, cfg, "SSPRK2", steps, 0.5, log_dt=False)
+    e[1].record()
+    s = st.to_numpy()
+    abar = raw.clone()
+    for f in raw.PLANES:
+        getattr(abar, f).zero_()
+    g = np.zeros_like(s["z_b"])
+    g[1:-1, 1:-1] = 2.0 * (s["z"] + s["z_b"] - target)[1:-1, 1:-1]
+    abar.z_b.copy_(torch.from_numpy(g))
+    pa = ParamAdjoints(cfg, raw.seds)
+    torch.cuda.synchronize()
+    e[2].record()
+    vjp_run(st0, abar, mask, cfg, steps, "SSPRK2", 0.5, checkpoint_every=every, params=pa)
+    vjp_init(raw, abar, mask, cfg, params=pa)
+    e[3].record()
+    e[3].synchronize()
+    fwd, bwd = e[0].elapsed_time(e[1]) / steps, e[2].elapsed_time(e[3]) / steps
+    return {"workload": f"roe_exner_inflow_{n}x{n}_mpm_ssprk2_f64_adjoint", "steps": steps,
+            "checkpoint_every": every, "forward_ms_per_step": fwd, "backward_ms_per_step": bwd,
+            "backward_over_forward": bwd / fwd,
+            "note": "backward: checkpointed forward recomputation + reverse sweep with the discharge and "
+                    "sediment-matrix adjoints, float64"}
+
+
 def plain_roe_run(steps=200, cpu_steps=10):
     """The plain Roe dam-break, 256 x 256 cells, float64, SSPRK2, 200
     steps through ``run_steps`` (graph replay), and the float64 NumPy oracle on the host
@@ -604,6 +649,8 @@ def main():
     ap.add_argument("--transport-u", type=float, default=1.0,
                     help="initial velocity of the bedload-everywhere variant of the case (0 to skip)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--adjoint-steps", type=int, default=64,
+                    help="steps of the configuration-4 reverse-mode timing (0 to skip)")
     ap.add_argument("--ensemble-members", type=int, default=64, help="ragged ensemble size (0 to skip)")
     ap.add_argument("--ensemble-steps", type=int, default=1000)
     ap.add_argument("--profile", action="store_true",
@@ -717,6 +764,7 @@ def main():
     ens = (ensemble_run(args.ensemble_members, args.ensemble_steps, world=world, rank=rank)
            if args.ensemble_members > 0 else None)
     roe = plain_roe_run() if rank == 0 and not args.no_cpu else None
+    adj = adjoint_run(steps=args.adjoint_steps) if rank == 0 and args.adjoint_steps > 0 else None
     acc = (accuracy_run(n, args.accuracy_steps, args.oracle_n, oracle_proc, oracle_path)
            if args.accuracy_steps > 0 else None)
     if rank != 0:
@@ -740,6 +788,7 @@ def main():
         "transport_case": transport,
         "ensemble": ens,
         "plain_roe": roe,
+        "adjoint": adj,
         "accuracy": acc,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,

@@ -110,6 +110,25 @@ def gaussian_bed(n, dx=0.01, seed_bed=1, seed_noise=2, device=None, u0=0.1):
                 boundaries=BoundaryManager(params, X, Y), X=X, Y=Y)
 
 
+def adjoint_case(n=512, q_in=0.3, seed_initial=1, seed_target=2, dx=0.01):
+    """Configuration 4: the Gaussian-bed generator at n x n (seed ``seed_initial``) started
+    at 1 m/s, a ConstantInflux inlet of ``q_in`` m^2/s (values [q_in, 1, 0]) with
+    TransmissiveBed on the left, Transmissive + TransmissiveBed on the right, Reflective in
+    y (MPM, one sediment), and the target total bed z_t of the same generator with seed
+    ``seed_target``.  Returns (arrs, params, X, Y, target)."""
+    import copy
+
+    ny = nx = n + 2
+    arrs = gaussian_bed_fields(n, dx, seed_bed=seed_initial, u0=1.0)
+    target = gaussian_bed_total(n, n, dx, seed_bed=seed_target)
+    bspec = ring_boundaries(ny, nx, [("ConstantInflux", [q_in, 1.0, 0.0, 0.0]), "TransmissiveBed"],
+                            ["Transmissive", "TransmissiveBed"], ["Reflective"], ["Reflective"])
+    erosion = dict(grass_factor="MPM", bulk_porosity=0.42, sediments=copy.deepcopy(SED_ONE))
+    params = dict(flux_scheme="Roe Exner", integrator="SSPRK2", cfl=0.5, erosion=erosion, boundaries=bspec)
+    X, Y = index_coords(ny, nx)
+    return arrs, params, X, Y, target
+
+
 # ------------------------------------------------------------------ Berthon analytic case
 BERTHON = dict(q=1.0, A=0.005, alpha=0.005, beta=0.005, gamma=1.0)
 

@@ -54,7 +54,7 @@ struct CflArgs {
 // Rows in flight ahead of the one the float32 CFL item evaluates (tuning knob; the item
 // does little arithmetic per row, so the copies must cover the memory latency).
 #ifndef PXB_CFL_AHEAD
-#define PXB_CFL_AHEAD 4
+#define PXB_CFL_AHEAD 2
 #endif
 
 // Float32 work item of the CFL reduction (a 31-column strip of one band; the 32nd lane

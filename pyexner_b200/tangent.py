@@ -157,27 +157,68 @@ def _adj_fields(abar):
     return abar.c_fields()
 
 
-def vjp_run(state0, abar, mask, solver_config, n_steps, scheme="SSPRK2", cfl=0.5, t0=0.0, checkpoint_every=32):
+class ParamAdjoints:
+    """Adjoints of the scalar parameters, accumulated by ``vjp_run`` / ``vjp_init`` with
+    ``params=``: ``seds_bar`` (7 x nsed like the state's ``seds``: dJ/d of the sediment
+    matrix of pnetcdf_reader.py:136-158; row 1 is the grain diameter d50) and
+    ``inflow_bar`` (boundary name -> dJ/d values[0], the discharge of each ConstantInflux
+    handler).  The reverse-mode counterpart of ``jvp_run``'s ``seds_dot`` / ``inflow_dot``."""
+
+    def __init__(self, solver_config, seds):
+        handlers = solver_config.boundaries.handlers if solver_config.boundaries is not None else []
+        self.names = [hd["name"] for hd in handlers]
+        self.seds_bar = np.zeros(np.asarray(seds).shape, dtype=np.float64)
+        self.values0_bar = np.zeros(max(1, len(self.names)), dtype=np.float64)
+
+    @property
+    def inflow_bar(self):
+        return {n: float(v) for n, v in zip(self.names, self.values0_bar)}
+
+    def _c(self):
+        self.seds_bar = np.ascontiguousarray(self.seds_bar)
+        p = _lib.ParamAdjoints()
+        p.seds_bar = self.seds_bar.ctypes.data
+        p.values0_bar = self.values0_bar.ctypes.data
+        return p
+
+
+def vjp_run(state0, abar, mask, solver_config, n_steps, scheme="SSPRK2", cfl=0.5, t0=0.0, checkpoint_every=32,
+            params=None):
     """Reverse mode of ``n_steps`` fixed steps from ``state0`` (the state after init, not
     modified): ``abar`` (a RoeExnerState whose h, hu, hv, z_b, G hold dJ/du of the final
     state) is overwritten IN PLACE with dJ/du of ``state0``.  The run is redone forward
-    with a checkpoint every ``checkpoint_every`` steps and undone segment by segment."""
+    with a checkpoint every ``checkpoint_every`` steps and undone segment by segment.
+    ``params`` (a ParamAdjoints): also accumulate the parameter adjoints; then ``abar.n_b``
+    (dJ/dn_b of the final state, n_b being constant) receives dJ/dn_b of ``state0``."""
     _check(state0, abar)
     plan = _re_plan(state0, mask, solver_config)
-    _lib.call("pxb_re_vjp_run", plan.handle, ctypes.byref(state0.c_fields()), int(n_steps),
-              _lib.SSPRK2 if scheme == "SSPRK2" else _lib.FE, float(cfl), float(t0), int(checkpoint_every),
-              ctypes.byref(_adj_fields(abar)), _stream())
+    code = _lib.SSPRK2 if scheme == "SSPRK2" else _lib.FE
+    if params is None:
+        _lib.call("pxb_re_vjp_run", plan.handle, ctypes.byref(state0.c_fields()), int(n_steps), code, float(cfl),
+                  float(t0), int(checkpoint_every), ctypes.byref(_adj_fields(abar)), _stream())
+    else:
+        p = params._c()
+        _lib.call("pxb_re_vjp_run_params", plan.handle, ctypes.byref(state0.c_fields()), int(n_steps), code,
+                  float(cfl), float(t0), int(checkpoint_every), ctypes.byref(_adj_fields(abar)), ctypes.byref(p),
+                  _stream())
     return abar
 
 
-def vjp_init(state_raw, abar, mask, solver_config):
+def vjp_init(state_raw, abar, mask, solver_config, params=None):
     """Reverse mode of init_fn_roeexner: ``abar`` (adjoint of the state after init) is
-    overwritten IN PLACE with the adjoint of ``state_raw`` (the state before init)."""
+    overwritten IN PLACE with the adjoint of ``state_raw`` (the state before init).  With
+    ``params``: also the parameter adjoints of the init, and ``abar.n_b`` (dJ/dn_b after
+    init) goes through compute_n to ``abar.n`` and to the sediment matrix."""
     _check(state_raw, abar)
     plan = _re_plan(state_raw, mask, solver_config)
-    _lib.call("pxb_re_vjp_init", plan.handle, ctypes.byref(state_raw.c_fields()), ctypes.byref(_adj_fields(abar)),
-              _stream())
+    if params is None:
+        _lib.call("pxb_re_vjp_init", plan.handle, ctypes.byref(state_raw.c_fields()),
+                  ctypes.byref(_adj_fields(abar)), _stream())
+    else:
+        p = params._c()
+        _lib.call("pxb_re_vjp_init_params", plan.handle, ctypes.byref(state_raw.c_fields()),
+                  ctypes.byref(_adj_fields(abar)), ctypes.byref(p), _stream())
     return abar
 
 
-__all__ += ["vjp_run", "vjp_init"]
+__all__ += ["vjp_run", "vjp_init", "ParamAdjoints"]
