@@ -202,8 +202,8 @@ int pxb_re_run(pxb_re_plan* plan, const pxb_re_fields* a, const pxb_re_fields* b
  * each stage adds dt dx times its boundary sum, times 1/2 under SSPRK2.  Then
  * volume(end) - volume(start) + outflow vanishes to rounding.  Fused stage path only
  * (PXB_ERR_UNSUPPORTED otherwise); acc_dev = NULL switches it off.  The first call with
- * an accumulator allocates the per-item partial array (16 bytes per work item of the
- * shortest band geometry). */
+ * an accumulator allocates the per-item partial array (16 bytes per work item of
+ * one-row bands, the most items a band geometry can have). */
 int pxb_re_volume(pxb_re_plan* plan, const pxb_re_fields* f, double* volumes, void* stream);
 int pxb_re_set_budget(pxb_re_plan* plan, double* acc_dev);
 

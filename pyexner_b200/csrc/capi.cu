@@ -802,7 +802,8 @@ int re_stage_impl(pxb_re_plan* P, const pxb_re_fields* in, const pxb_re_fields* 
     a.err = &P->c.scr->err;
     a.queue = P->c.scr->queue;
     const long long nitems = (long long)pxb_stage_items_per_band(g.nstrips) * g.nbands;
-    const bool bud = bud_w > 0.0 && P->bud_acc && P->bud_part && nitems <= P->bud_items;
+    const bool bud = bud_w > 0.0 && P->bud_acc && P->bud_part;
+    if (bud && nitems > P->bud_items) return fail(PXB_ERR_ARG, "budget partials smaller than the band geometry");
     if (bud) a.bud = P->bud_part;
     PXB_CUDA(pxb::launch_re_stage<T>(a, P->mpm != 0, P->nodata != nullptr, avg != nullptr, g.grid, s));
     if (bud)
@@ -2195,10 +2196,10 @@ int pxb_re_set_budget(pxb_re_plan* P, double* acc_dev) {
         return fail(PXB_ERR_UNSUPPORTED, "the volume budget is built into the fused stage path only");
     if (acc_dev && ((uintptr_t)acc_dev & 7u)) return fail(PXB_ERR_ARG, "acc_dev must be 8-byte aligned");
     if (acc_dev && !P->bud_part) {
-        // every band height the plan can take (the autotuner goes down to 8 rows)
+        // every band geometry the plan can take: bands of one row at least
         const int nstrips = std::max(1, (P->c.nx - 3 + pxb_stage_strip_out((int)P->c.esize()) - 1) /
                                             pxb_stage_strip_out((int)P->c.esize()));
-        const long long items = (long long)pxb_stage_items_per_band(nstrips) * ((P->c.ny - 1 + 7) / 8 + 1);
+        const long long items = (long long)pxb_stage_items_per_band(nstrips) * P->c.ny;
         PXB_CUDA(cudaMalloc(&P->bud_part, sizeof(double) * 2 * (size_t)items));
         P->bud_items = items;
     }
