@@ -13,8 +13,6 @@
 // Work layout: a warp covers 32 columns and the 31 x-faces between them (strips overlap
 // by one column) and marches down a band of rows; y-faces (r | r+1) belong to row r's band.
 #pragma once
-#include <type_traits>
-
 #include "pxb_device.cuh"
 #include "re_stage.cuh"  // cp.async helpers
 
@@ -72,13 +70,6 @@ struct CflArgs {
 constexpr int PXB_CFL_RW = 36;  // floats per plane row in a shared slot of the float32 CFL item
 constexpr int PXB_CFL_SLOTS = PXB_CFL_AHEAD < 4 ? 4 : (PXB_CFL_AHEAD < 8 ? 8 : 16);  // a power of two above AHEAD
 
-// A slot index given as an int or as a std::integral_constant (compile-time).
-template <class S>
-__device__ __forceinline__ constexpr int cfl_slot(S s) {
-    if constexpr (std::is_integral<S>::value) return s;
-    else return S::value;
-}
-
 // cb: this warp's slots (PXB_CFL_SLOTS rows of the four planes, PXB_CFL_RW floats each)
 template <bool HAS_MASK, bool VEC>
 __device__ __forceinline__ void re_cfl_item_f32(const CflArgs<float>& a, const int item, unsigned& best,
@@ -116,24 +107,20 @@ __device__ __forceinline__ void re_cfl_item_f32(const CflArgs<float>& a, const i
         cdst[q] = (unsigned)__cvta_generic_to_shared(&cb[0][pl][4 * (j < 9 ? j : 0)]);
     }
     constexpr unsigned SLOT = 4 * RW * sizeof(float);
-    // Rows live in slot (r - R0) % SLOTS: in the steady loop below, which takes four rows
-    // per iteration, every slot index is a compile-time constant.  Rows at or beyond rend
-    // are issued as zero-byte copies of the last row (no branch).
-    const unsigned rlast = (unsigned)(rend - 1) * upitch;
-    auto issue = [&](int rr, int slot) __attribute__((always_inline)) {
-        const unsigned so = (unsigned)slot * SLOT;
-        if constexpr (VEC) {
-            const bool rok = rr < rend;
-            const unsigned ro = rok ? (unsigned)rr * upitch : rlast;
-            cp_async16_zfill(cdst[0] + so, csrc[0] + ro, rok ? cbytes[0] : 0u);
-            if (lane < 4) cp_async16_zfill(cdst[1] + so, csrc[1] + ro, rok ? cbytes[1] : 0u);
-        } else if (colok && rr < rend) {
+    auto issue = [&](int rr) __attribute__((always_inline)) {  // row rr into slot rr % SLOTS
+        if (rr < rend) {
             const unsigned ro = (unsigned)rr * upitch;
-            float* d = &cb[0][0][lane] + slot * (SLOT / sizeof(float));
-            cp_async_elem(d, a.h + ro + c);
-            cp_async_elem(d + RW, a.hu + ro + c);
-            cp_async_elem(d + 2 * RW, a.hv + ro + c);
-            cp_async_elem(d + 3 * RW, a.G + ro + c);
+            const unsigned so = (unsigned)(rr & (SLOTS - 1)) * SLOT;
+            if constexpr (VEC) {
+                cp_async16_zfill(cdst[0] + so, csrc[0] + ro, cbytes[0]);
+                if (lane < 4) cp_async16_zfill(cdst[1] + so, csrc[1] + ro, cbytes[1]);
+            } else if (colok) {
+                float* d = &cb[rr & (SLOTS - 1)][0][lane];
+                cp_async_elem(d, a.h + ro + c);
+                cp_async_elem(d + RW, a.hu + ro + c);
+                cp_async_elem(d + 2 * RW, a.hv + ro + c);
+                cp_async_elem(d + 3 * RW, a.G + ro + c);
+            }
         }
         cp_async_commit();
     };
@@ -142,24 +129,21 @@ __device__ __forceinline__ void re_cfl_item_f32(const CflArgs<float>& a, const i
         nm = false;
         if (HAS_MASK && colok && rr < rend) nm = __ldg(a.nodata + (unsigned)rr * upitch + (unsigned)c) != 0;
     };
-    // One row r (in slot `slot`): its x-faces when XF, the y-faces (r-1 | r) when YF.
-    auto row = [&](const int r, auto slot_tag, auto xf_tag, auto yf_tag, CCell<float>& cur, bool& mc,
-                   const CCell<float>& prev, const bool mp) __attribute__((always_inline)) {
-        constexpr bool XF = decltype(xf_tag)::value, YF = decltype(yf_tag)::value;
-        const int slot = cfl_slot(slot_tag);
+    auto row = [&](const int r, CCell<float>& cur, bool& mc, const CCell<float>& prev, const bool mp)
+                   __attribute__((always_inline)) {
         cp_async_wait<AHEAD - 1>();  // row r landed (rows r+1 .. r+AHEAD-1 may be in flight)
         if constexpr (VEC) __syncwarp();  // chunks copied by other lanes
-        const float* sr = &cb[0][0][off + lane] + slot * (SLOT / sizeof(float));
+        const float* sr = &cb[r & (SLOTS - 1)][0][off + lane];
         const float h = sr[0], hu = sr[RW], hv = sr[2 * RW];
         const float g = colok ? sr[3 * RW] : 0.f;
-        issue(r + AHEAD, (slot + AHEAD) & (SLOTS - 1));
+        issue(r + AHEAD);
         mc = nm;
         fetch_mask(r + 1);
         cur = make_ccell(h, hu, hv, g);
         // rows r-1 and r of the warp without G (below the Shields threshold) take
         // face_speed_nog, the same value without a~ and the cubic (a NaN G is not 0)
-        const bool nog = !__any_sync(FULL, !(g == 0.f) || (YF && !(prev.G == 0.f)));
-        if constexpr (XF) {  // x-face (c | c+1) of row r
+        const bool nog = !__any_sync(FULL, !(g == 0.f) || !(prev.G == 0.f));
+        if (r < R1) {  // x-face (c | c+1) of row r
             CCell<float> e;
             e.h = __shfl_down_sync(FULL, cur.h, 1);
             e.sq = __shfl_down_sync(FULL, cur.sq, 1);
@@ -182,7 +166,7 @@ __device__ __forceinline__ void re_cfl_item_f32(const CflArgs<float>& a, const i
                 }
             }
         }
-        if constexpr (YF) {  // y-face (r-1 | r)
+        if (r > R0) {  // y-face (r-1 | r)
             const bool act = colok && ((prev.h > DRY) || (cur.h > DRY)) && !(mp || mc);
             if (nog) {
                 const unsigned b = __float_as_uint(face_speed_nog<float, true>(prev, cur));
@@ -193,38 +177,17 @@ __device__ __forceinline__ void re_cfl_item_f32(const CflArgs<float>& a, const i
             }
         }
     };
-    using T_ = std::true_type;
-    using F_ = std::false_type;
-    using I0 = std::integral_constant<int, 0>;
-    using I1 = std::integral_constant<int, 1>;
-    using I2 = std::integral_constant<int, 2>;
-    using I3 = std::integral_constant<int, 3>;
-    static_assert(SLOTS == 4 || AHEAD >= 4, "the steady loop's slot constants assume four slots");
 #pragma unroll
-    for (int k = 0; k < AHEAD; ++k) issue(R0 + k, k & (SLOTS - 1));
+    for (int k = 0; k < AHEAD; ++k) issue(R0 + k);
     fetch_mask(R0);
     CCell<float> pa = make_ccell(1.f, 0.f, 0.f, 0.f), pb = pa;
     bool ma = false, mb = false;
-    // prologue: row R0, x-faces only (a band has at least one row)
-    row(R0, I0{}, T_{}, F_{}, pa, ma, pb, mb);
-    int r = R0 + 1;
-    if constexpr (SLOTS == 4) {
-        // steady state: rows R0+1 .. R1-1, both faces, four rows per iteration
-        for (; r + 3 < R1; r += 4) {
-            row(r, I1{}, T_{}, T_{}, pb, mb, pa, ma);
-            row(r + 1, I2{}, T_{}, T_{}, pa, ma, pb, mb);
-            row(r + 2, I3{}, T_{}, T_{}, pb, mb, pa, ma);
-            row(r + 3, I0{}, T_{}, T_{}, pa, ma, pb, mb);
-        }
+    int r = R0;
+    for (; r + 1 < rend; r += 2) {
+        row(r, pb, mb, pa, ma);
+        row(r + 1, pa, ma, pb, mb);
     }
-    // the rest of the band (runtime slots), the current cell always in pa
-    for (; r < R1; ++r) {
-        row(r, (r - R0) & (SLOTS - 1), T_{}, T_{}, pb, mb, pa, ma);
-        pa = pb;
-        ma = mb;
-    }
-    // epilogue: row R1 (the first of the next band), y-faces (R1-1 | R1) only
-    if (R1 < rend) row(R1, (R1 - R0) & (SLOTS - 1), F_{}, T_{}, pb, mb, pa, ma);
+    if (r < rend) row(r, pb, mb, pa, ma);
     cp_async_wait<0>();  // the slots are reused by the next item
     __syncwarp();
 }
@@ -349,15 +312,8 @@ __device__ __forceinline__ void re_cfl_item(const CflArgs<T>& a, const int item,
   }
 }
 
-// Resident 256-thread blocks per SM the float32 CFL kernel is register-limited to (tuning
-// knob; 0 leaves the register count to the compiler).
-#ifndef PXB_CFL_MIN_BLOCKS_F32
-#define PXB_CFL_MIN_BLOCKS_F32 0
-#endif
-#define PXB_CFL_BOUNDS(T) ((sizeof(T) == 4 && PXB_CFL_MIN_BLOCKS_F32 > 0) ? PXB_CFL_MIN_BLOCKS_F32 : 1)
-
 template <class T, bool HAS_MASK>
-__global__ void __launch_bounds__(256, PXB_CFL_BOUNDS(T)) re_cfl_kernel(const CflArgs<T> a) {
+__global__ void __launch_bounds__(256) re_cfl_kernel(const CflArgs<T> a) {
     const int lane = threadIdx.x & 31;
     const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;

@@ -324,3 +324,38 @@ def test_mixed_bedload_regions(dtype):
     tolN = TOL[dtype][1]
     assert rel_err(dts.cpu().numpy(), odts) <= tolN
     assert_planes(st.to_numpy(), orun, tolN, what="ssprk2")
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32], ids=["f64", "f32"])
+@pytest.mark.parametrize("shape", [(3, 3), (4, 5), (200, 3), (3, 200), (5, 257), (41, 27)],
+                         ids=["3x3", "4x5", "200x3", "3x200", "5x257", "41x27"])
+@pytest.mark.parametrize("bc", ["trans_x_refl_y", "refl_all"])
+def test_roe_exner_extreme_shapes(shape, bc, dtype):
+    """The smallest grid the plans accept (3 x 3, ring included), grids with one physical
+    row or column (every cell a ring cell or a neighbour of one), 257 columns (ten float32
+    strips of 26 owned columns, the last one short) and bands of 4 rows, so that most items
+    are shorter than the pipeline's depth: init, dt, one stage and 4 SSPRK2 steps against
+    the oracle."""
+    from pyexner_b200 import run_steps
+    from pyexner_b200.cases import seds_matrix
+
+    ny, nx = shape
+    arrs, params, X, Y, mpm = random_re_case(ny, nx, seed=ny * 7 + nx, regime="smooth", bcname=bc)
+    params["band_rows"] = 4
+    seds = seds_matrix(params["erosion"])
+    dx = 0.1
+    ost, omask, obcs = oracle_setup(arrs, params, X, Y, mpm, seds)
+    odt = ORE.compute_dt(ost, 0.5, dx, omask[0])
+    o1 = ORE.stage(ost, odt, dx, omask, obcs, mpm)
+    orun, odts = OI.run_roe_exner(ost, omask, obcs, mpm, dx, 0.5, 4, "SSPRK2")
+    tol1, tolN = TOL[dtype]
+    g_tol = 2e-4 if dtype == torch.float32 else None
+    bundle, cfg, mask, st = device_re(arrs, params, X, Y, seds, dtype, dx)
+    assert_planes(st.to_numpy(), ost, tol1, what="init", g_tol=g_tol)
+    assert rel_err(float(bundle.compute_dt_fn(st, 0.5, mask, cfg)), float(odt)) <= tol1
+    s1 = bundle.step_fn(st, 0.0, float(odt), mask, cfg)
+    assert_planes(s1.to_numpy(), o1, tol1, what="stage", g_tol=g_tol)
+    s = st.clone()
+    dts = run_steps(s, mask, cfg, "SSPRK2", 4, 0.5)
+    assert rel_err(dts.cpu().numpy(), odts) <= tolN
+    assert_planes(s.to_numpy(), orun, tolN, what="ssprk2")
