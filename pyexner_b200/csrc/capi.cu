@@ -765,7 +765,7 @@ int re_cfl_impl(pxb_re_plan* P, const pxb_re_fields* f, double cfl, void* dt_out
 
 template <class T>
 int re_stage_impl(pxb_re_plan* P, const pxb_re_fields* in, const pxb_re_fields* out, const pxb_re_fields* avg,
-                  const void* dt, cudaStream_t s, double bud_w = 0.0, double next_cfl = 0.0, void* dt_log = nullptr) {
+                  const void* dt, cudaStream_t s, double bud_w = 0.0) {
     pxb::REStageArgs<T> a{};
     a.ny = P->c.ny;
     a.nx = P->c.nx;
@@ -805,16 +805,6 @@ int re_stage_impl(pxb_re_plan* P, const pxb_re_fields* in, const pxb_re_fields* 
     const bool bud = bud_w > 0.0 && P->bud_acc && P->bud_part;
     if (bud && nitems > P->bud_items) return fail(PXB_ERR_ARG, "budget partials smaller than the band geometry");
     if (bud) a.bud = P->bud_part;
-    if (next_cfl > 0.0) {
-        // the averaging stage also takes the next step's dt from its output, into the plan's
-        // time step and the dt log, as re_cfl_impl on the stored state would
-        if (!avg || bud) return fail(PXB_ERR_ARG, "the next time step is taken by the averaging stage, without budget");
-        a.cscr = P->c.scr;
-        a.cfl = (T)next_cfl;
-        a.cfl_floor = (T)pxb::DT_FLOOR;
-        a.cfl_dt_out = (T*)P->c.dt_dev;
-        a.cfl_dt_log = (T*)dt_log;
-    }
     PXB_CUDA(pxb::launch_re_stage<T>(a, P->mpm != 0, P->nodata != nullptr, avg != nullptr, g.grid, s));
     if (bud)
         PXB_CUDA(pxb::launch_budget_stage<T>(P->bud_part, (int)nitems, (const T*)dt, bud_w * P->c.dx, P->bud_acc, s));
@@ -1055,27 +1045,6 @@ int re_steps(pxb_re_plan* P, const pxb_re_fields* A, const pxb_re_fields* B, int
     if (scheme == PXB_SSPRK2) {
         pxb_re_fields B1 = Bs;
         if (P->mpm) B1.G = nullptr;  // stage-1 G is recomputed by stage 2
-        if (!general && bud_w == 0.0 && nsteps > 1) {
-            // The first step's dt from the CFL kernel; then every averaging stage but the
-            // last takes the next step's dt from its own output (one launch fewer per step,
-            // the same dt bit for bit); the last step's averaging stage takes none, so the dt
-            // log holds exactly nsteps entries.
-            auto fused_stage2 = [&](cudaStream_t st) {
-                return f64 ? re_stage_impl<double>(P, &Bs, A, A, P->c.dt_dev, st, 0.0, cfl, dt_log)
-                           : re_stage_impl<float>(P, &Bs, A, A, P->c.dt_dev, st, 0.0, cfl, dt_log);
-            };
-            int r = cfl_call(A, s);
-            if (r != PXB_OK) return r;
-            key.push_back((const void*)(intptr_t)1);  // the fused body
-            r = run_graph(P->c, key, nsteps - 1, s, [&](cudaStream_t st) {
-                int q = stage_call(A, &B1, nullptr, st);
-                if (q == PXB_OK) q = fused_stage2(st);
-                return q;
-            });
-            if (r == PXB_OK) r = stage_call(A, &B1, nullptr, s);
-            if (r == PXB_OK) r = stage_call(&Bs, A, A, s);
-            return r;
-        }
         return run_graph(P->c, key, nsteps, s, [&](cudaStream_t st) {
             int r = cfl_call(A, st);
             if (r == PXB_OK) r = stage_call(A, &B1, nullptr, st);

@@ -6,15 +6,9 @@ namespace pxb {
 
 template <class T, bool MPM, bool HM, bool AVG>
 static cudaError_t stage_variant(const REStageArgs<T>& a, int grid, cudaStream_t s) {
-    // the budget variant only when its partial array is set, the variant that also takes the
-    // next step's time step only when its scratch is (the others carry none of their code)
+    // the budget variant only when its partial array is set (the others carry no budget code)
     if (a.bud) re_stage_kernel<T, MPM, HM, AVG, true><<<grid, 128, 0, s>>>(a);
-    else if constexpr (AVG) {
-        if (a.cscr) re_stage_kernel<T, MPM, HM, AVG, false, true><<<grid, 128, 0, s>>>(a);
-        else re_stage_kernel<T, MPM, HM, AVG, false, false><<<grid, 128, 0, s>>>(a);
-    } else {
-        re_stage_kernel<T, MPM, HM, AVG, false><<<grid, 128, 0, s>>>(a);
-    }
+    else re_stage_kernel<T, MPM, HM, AVG, false><<<grid, 128, 0, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -18,6 +18,19 @@
 
 namespace pxb {
 
+struct CflScratch {
+    unsigned long long maxbits;  // running max of speed bits
+    unsigned int done;           // finished blocks of the current launch
+    unsigned int step;           // index into the dt log
+    int err;                     // sticky error word
+    int pad;
+    double t_step;               // simulation time at the start of the current step
+    double t_next;               // t_step + dt: the time the next dt is added to
+    unsigned int queue[2];       // stage kernel work queue: items handed out, blocks finished
+    unsigned int cfl_queue;      // CFL kernel work queue: items handed out (reset by the last block)
+    unsigned int pad2;
+};
+
 // Start of a fixed-step run at time t0 (the first CFL launch moves it into t_step).
 template <class T>
 __global__ void set_time_kernel(CflScratch* scr, double t0) {
@@ -331,7 +344,19 @@ __global__ void __launch_bounds__(256) re_cfl_kernel(const CflArgs<T> a) {
     const unsigned int ticket = atomicAdd(&a.scr->done, 1u);
     if (ticket == gridDim.x - 1) {
         __threadfence();
-        cfl_finalize<T>(a.scr, atomicAdd(&a.scr->maxbits, 0ull), a.cfl, a.dx, a.floor_dt, a.dt_out, a.dt_log);
+        const unsigned long long bits = atomicAdd(&a.scr->maxbits, 0ull);
+        const T smax = bits_speed(bits, T(0));
+        // min_f dx/speed_f (inf when no face is active), then cfl * dt and the floor
+        T dt = a.cfl * (a.dx / smax);
+        if (a.floor_dt > T(0)) dt = clamp_lo(dt, a.floor_dt);
+        *a.dt_out = dt;
+        if (a.dt_log) a.dt_log[a.scr->step] = dt;
+        a.scr->step += 1;
+        // time of this step, accumulated in float64 like the host loops of the integrators
+        a.scr->t_step = a.scr->t_next;
+        a.scr->t_next = a.scr->t_next + (double)dt;
+        if (!d_isfinite(dt)) a.scr->err |= 2;
+        a.scr->maxbits = 0ull;
         a.scr->done = 0u;
         a.scr->cfl_queue = 0u;  // every warp has left its item loop
         __threadfence();

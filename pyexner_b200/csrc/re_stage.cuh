@@ -58,41 +58,6 @@
 
 namespace pxb {
 
-// Device scratch of a plan's time step (the CFL kernels and the averaging stage that
-// computes the next step's dt).
-struct CflScratch {
-    unsigned long long maxbits;  // running max of speed bits
-    unsigned int done;           // finished blocks of the current launch
-    unsigned int step;           // index into the dt log
-    int err;                     // sticky error word
-    int pad;
-    double t_step;               // simulation time at the start of the current step
-    double t_next;               // t_step + dt: the time the next dt is added to
-    unsigned int queue[2];       // stage kernel work queue: items handed out, blocks finished
-    unsigned int cfl_queue;      // CFL kernel work queue: items handed out (reset by the last block)
-    unsigned int pad2;
-};
-
-// The end of a CFL reduction, run once by the last block: dt = max(cfl * dx / smax,
-// floor) from the bit pattern of the largest face speed (min_f dx / speed_f, inf when no
-// face is active), written to dt_out and to the dt log; advances the step index and the
-// step's simulation time (float64, like the host loops of the integrators), flags a
-// non-finite dt, and clears the running maximum.
-template <class T>
-__device__ __forceinline__ void cfl_finalize(CflScratch* scr, unsigned long long bits, T cfl, T dx, T floor_dt,
-                                             T* dt_out, T* dt_log) {
-    const T smax = bits_speed(bits, T(0));
-    T dt = cfl * (dx / smax);
-    if (floor_dt > T(0)) dt = clamp_lo(dt, floor_dt);
-    *dt_out = dt;
-    if (dt_log) dt_log[scr->step] = dt;
-    scr->step += 1;
-    scr->t_step = scr->t_next;
-    scr->t_next = scr->t_next + (double)dt;
-    if (!d_isfinite(dt)) scr->err |= 2;
-    scr->maxbits = 0ull;
-}
-
 template <class T>
 struct REStageArgs {
     int ny, nx;
@@ -113,13 +78,6 @@ struct REStageArgs {
     // the boundary faces) and of sediment (Exner fluxes), in the state's flux units; item
     // k writes bud[2k], bud[2k+1] on every launch.
     double* bud;
-    // Next step's time step (the CFL instantiation of the averaging stage): the face speeds
-    // of the stage's output, reduced like re_cfl_kernel and finalised by the last block into
-    // cfl_dt_out / cfl_dt_log through cscr.
-    CflScratch* cscr;
-    T cfl, cfl_floor;
-    T* cfl_dt_out;
-    T* cfl_dt_log;
 };
 
 // Asynchronous global -> shared copies of one element (cp.async, completion by group).
@@ -243,15 +201,8 @@ __device__ __forceinline__ void read_cols(const T* rowp, int lane, T (&v)[CPT]) 
 // consecutive columns (pxb_stage_cpt): a strip is 32 * CPT columns, 3 halo | owned | 3
 // halo.  Neighbour values inside a lane are plain registers; across lanes one shuffle
 // moves the first (east) or last (west) column.
-// CFL (averaging stage only): also the largest face speed of the stage's output over the
-// faces the item owns (x-faces of its rows and columns, y-faces (p-1 | p) of its rows),
-// folded into *cbest: the time step of the next step, as re_cfl_item would take it from the
-// stored state.  The averaged state is formed for one more column (the east neighbour of
-// the last owned one) and one more row (the one above the band) than are stored.
-template <class T, bool MPM, bool HAS_MASK, bool AVG, bool BUD = false, bool CFL = false>
-__device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int item, bool& bad,
-                                              unsigned long long* cbest = nullptr) {
-    static_assert(!CFL || AVG, "the next step's time step is taken by the averaging stage");
+template <class T, bool MPM, bool HAS_MASK, bool AVG, bool BUD = false>
+__device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int item, bool& bad) {
     constexpr int CPT = pxb_stage_cpt((int)sizeof(T));
     constexpr int W = 32 * CPT;
     const int lane = threadIdx.x & 31;
@@ -271,7 +222,7 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
         else if (kb >= a.nstrips) { strip = a.nstrips - 1; half = kb - a.nstrips; }
         const bool last_strip = strip == a.nstrips - 1;
         const int cb = strip * (W - 2 * PXB_HALO) - PXB_HALO + CPT * lane;  // column of this lane's first element
-        bool colok[CPT], has_e[CPT], out_col[CPT], interior_col[CPT], cfl_col[CPT];
+        bool colok[CPT], has_e[CPT], out_col[CPT], interior_col[CPT];
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
             const int c = cb + k, j = CPT * lane + k;
@@ -279,9 +230,6 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
             has_e[k] = colok[k] && (c + 1 < nx) && (j < W - 1);
             out_col[k] = colok[k] && j >= PXB_HALO && (j < W - PXB_HALO || last_strip);
             interior_col[k] = (c >= 1) && (c <= nx - 2);
-            // the owned columns and the east neighbour of the last one (valid: two columns
-            // inside the strip's halo, where every value of the stage is exact)
-            cfl_col[k] = colok[k] && j >= PXB_HALO && (j <= W - PXB_HALO || last_strip);
         }
         const int B0 = band * a.band_rows;
         const int B1 = (band == a.nbands - 1) ? ny : B0 + a.band_rows;
@@ -289,12 +237,6 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
         const int R0 = half == 1 ? Bm : B0;
         const int R1 = half == 0 ? Bm : B1;
         const int L0 = max(0, R0 - 3), L1 = min(ny, R1 + 3);
-        // rows and columns whose averaged (SSPRK2) output is formed: the stored ones, and
-        // for the next step's time step one more row above the band and one more column
-        const int A0 = CFL ? R0 - 1 : R0;
-        bool avg_col[CPT];
-#pragma unroll
-        for (int k = 0; k < CPT; ++k) avg_col[k] = CFL ? cfl_col[k] : out_col[k];
         // boundary recipes can only apply in the first/last strip or on rows 0 / ny-1
         const bool bc_strip = (a.ring != nullptr) && (strip == 0 || last_strip);
         const bool bc_rows = (a.ring != nullptr) && (R0 == 0 || R1 == ny);
@@ -325,18 +267,6 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
         ECell<T> e4[CPT];
         T xe4[CPT], fn4[CPT];
         T zbp6[CPT], zbp5[CPT], gg6[CPT], gg5[CPT];
-        // CFL: output h, hu, hv of rows r-4 (f1) and r-5 (f2); the output cell of the row above
-        // the one phase H treats, and its nodata flag
-        T f1h[CPT], f1u[CPT], f1v[CPT], f2h[CPT], f2u[CPT], f2v[CPT];
-        CCell<T> cprev[CPT];
-        bool mprev[CPT];
-#pragma unroll
-        for (int k = 0; k < CPT; ++k) {
-            f1h[k] = f2h[k] = T(1);
-            f1u[k] = f1v[k] = f2u[k] = f2v[k] = T(0);
-            cprev[k] = make_ccell(T(1), T(0), T(0), T(0));
-            mprev[k] = false;
-        }
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
             pA[k] = make_hcell(T(0), T(0), T(0), T(0), T(0), T(0));
@@ -424,13 +354,13 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
 #pragma unroll
             for (int k = 0; k < CPT; ++k) {
                 const int e = CPT * lane + k;
-                if (q0 >= L0 && q0 < L1 && q0 >= A0 && q0 < R1 && avg_col[k]) {
+                if (q0 >= L0 && q0 < L1 && q0 >= R0 && q0 < R1 && out_col[k]) {
                     const unsigned i = (unsigned)q0 * upitch + (unsigned)(cb + k);
                     cp_async_elem(&pb[b][0][e], a.ah + i);
                     cp_async_elem(&pb[b][1][e], a.ahu + i);
                     cp_async_elem(&pb[b][2][e], a.ahv + i);
                 }
-                if (p0 >= L0 && p0 < L1 && p0 >= A0 && p0 < R1 && avg_col[k]) {
+                if (p0 >= L0 && p0 < L1 && p0 >= R0 && p0 < R1 && out_col[k]) {
                     const unsigned i = (unsigned)p0 * upitch + (unsigned)(cb + k);
                     cp_async_elem(&pb[b][3][e], a.azb + i);
                     if (a.oG) cp_async_elem(&pb[b][4][e], a.aG + i);
@@ -512,13 +442,13 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
                 const int q0 = r - 3, p0 = r - 5;
 #pragma unroll
                 for (int k = 0; k < CPT; ++k) {
-                    if ((S || (q0 >= L0 && q0 < L1)) && q0 >= A0 && q0 < R1 && avg_col[k]) {
+                    if ((S || (q0 >= L0 && q0 < L1)) && q0 >= R0 && q0 < R1 && out_col[k]) {
                         const unsigned i = (unsigned)q0 * upitch + (unsigned)(cb + k);
                         pah[k] = a.ah[i];
                         pahu[k] = a.ahu[i];
                         pahv[k] = a.ahv[i];
                     }
-                    if ((S || (p0 >= L0 && p0 < L1)) && p0 >= A0 && p0 < R1 && avg_col[k]) {
+                    if ((S || (p0 >= L0 && p0 < L1)) && p0 >= R0 && p0 < R1 && out_col[k]) {
                         const unsigned i = (unsigned)p0 * upitch + (unsigned)(cb + k);
                         pazb[k] = a.azb[i];
                         if (a.oG) paG[k] = a.aG[i];
@@ -903,37 +833,26 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
                     }
                 }
             }
-            T gcfl[CPT];  // CFL: the output G of row p
-#pragma unroll
-            for (int k = 0; k < CPT; ++k) gcfl[k] = T(0);
-            if (rowG && p >= A0 && p < R1) {
+            if (rowG && p >= R0 && p < R1) {
                 if constexpr (ASYNC_PARTNER) {
                     read_cols<CPT>(pb[r & 1][3], lane, pazb);
                     if (a.oG) read_cols<CPT>(pb[r & 1][4], lane, paG);
                 }
 #pragma unroll
                 for (int k = 0; k < CPT; ++k) {
-                    if (!avg_col[k]) continue;
+                    if (!out_col[k]) continue;
                     const unsigned i = (unsigned)p * upitch + (unsigned)(cb + k);
                     T zo = zfin[k], go = gfin[k];
                     if (AVG) {
                         zo = T(0.5) * pazb[k] + T(0.5) * zo;
                         if (a.oG) go = T(0.5) * paG[k] + T(0.5) * go;
                     }
-                    gcfl[k] = go;
-                    if (CFL && !(out_col[k] && p >= R0)) continue;
                     a.ozb[i] = zo;
                     if (a.oG) a.oG[i] = go;
                     bad |= !d_isfinite(zo);
                 }
             }
-            T fqh[CPT], fqu[CPT], fqv[CPT];  // CFL: the output h, hu, hv of row q
-#pragma unroll
-            for (int k = 0; k < CPT; ++k) {
-                fqh[k] = T(1);
-                fqu[k] = fqv[k] = T(0);
-            }
-            if (rowD && q >= A0 && q < R1) {
+            if (rowD && q >= R0 && q < R1) {
                 if constexpr (ASYNC_PARTNER) {
                     read_cols<CPT>(pb[r & 1][0], lane, pah);
                     read_cols<CPT>(pb[r & 1][1], lane, pahu);
@@ -941,7 +860,7 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
                 }
 #pragma unroll
                 for (int k = 0; k < CPT; ++k) {
-                    if (!avg_col[k]) continue;
+                    if (!out_col[k]) continue;
                     const unsigned i = (unsigned)q * upitch + (unsigned)(cb + k);
                     T oh = sbh[k], ou = sbu[k], ov = sbv[k];
                     if (AVG) {
@@ -949,80 +868,10 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
                         ou = T(0.5) * pahu[k] + T(0.5) * ou;
                         ov = T(0.5) * pahv[k] + T(0.5) * ov;
                     }
-                    fqh[k] = oh;
-                    fqu[k] = ou;
-                    fqv[k] = ov;
-                    if (CFL && !(out_col[k] && q >= R0)) continue;
                     a.oh[i] = oh;
                     a.ohu[i] = ou;
                     a.ohv[i] = ov;
                     bad |= !(d_isfinite(oh) && d_isfinite(ou) && d_isfinite(ov));
-                }
-            }
-
-            // ================= H (CFL): face speeds of the output, row p
-            // The output h, hu, hv of row p were formed two iterations ago (f2*), its G just
-            // now; the row above is the previous iteration's cell (cprev).  Faces as
-            // re_cfl_item takes them: x-faces (p: c | c+1) of the owned columns, y-faces
-            // (p-1 | p), active where either side is wet and neither is nodata.
-            if constexpr (CFL) {
-                if (rowG && p >= A0 && p < R1) {
-                    const T DRYc = T(DRY_TOL);
-                    CCell<T> cur[CPT];
-                    bool mcur[CPT];
-#pragma unroll
-                    for (int k = 0; k < CPT; ++k) {
-                        cur[k] = avg_col[k] ? make_ccell(f2h[k], f2u[k], f2v[k], gcfl[k])
-                                            : make_ccell(T(1), T(0), T(0), T(0));
-                        mcur[k] = HAS_MASK && ((mwin[k] >> 4) & 1u);
-                    }
-                    if (p >= R0) {
-                        bool gany = false;
-#pragma unroll
-                        for (int k = 0; k < CPT; ++k) gany = gany || !(cur[k].G == T(0)) || !(cprev[k].G == T(0));
-                        const bool nog = !__any_sync(FULL, gany);
-                        CCell<T> ce[CPT];
-                        bool me[CPT];
-#pragma unroll
-                        for (int k = 0; k + 1 < CPT; ++k) { ce[k] = cur[k + 1]; me[k] = mcur[k + 1]; }
-                        ce[CPT - 1].h = __shfl_down_sync(FULL, cur[0].h, 1);
-                        ce[CPT - 1].sq = __shfl_down_sync(FULL, cur[0].sq, 1);
-                        ce[CPT - 1].u = __shfl_down_sync(FULL, cur[0].u, 1);
-                        ce[CPT - 1].v = __shfl_down_sync(FULL, cur[0].v, 1);
-                        me[CPT - 1] = HAS_MASK ? (__shfl_down_sync(FULL, (int)mcur[0], 1) != 0) : false;
-                        if (!nog) {
-                            ce[CPT - 1].G = __shfl_down_sync(FULL, cur[0].G, 1);
-                            ce[CPT - 1].rs = __shfl_down_sync(FULL, cur[0].rs, 1);
-                        }
-#pragma unroll
-                        for (int k = 0; k < CPT; ++k) {
-                            const bool xact = out_col[k] && has_e[k] && ((cur[k].h > DRYc) || (ce[k].h > DRYc)) &&
-                                              !(mcur[k] || me[k]);
-                            const bool yact = out_col[k] && p >= 1 && ((cprev[k].h > DRYc) || (cur[k].h > DRYc)) &&
-                                              !(mprev[k] || mcur[k]);
-                            if (nog) {
-                                const unsigned long long bx = speed_bits(face_speed_nog<T, false>(cur[k], ce[k]));
-                                const unsigned long long by = speed_bits(face_speed_nog<T, true>(cprev[k], cur[k]));
-                                if (xact && bx > *cbest) *cbest = bx;
-                                if (yact && by > *cbest) *cbest = by;
-                            } else {
-                                // only active faces enter the cubic (see re_cfl_item_f32)
-                                if (xact) {
-                                    const unsigned long long bx = speed_bits(face_speed<T, false>(cur[k], ce[k]));
-                                    if (bx > *cbest) *cbest = bx;
-                                }
-                                if (yact) {
-                                    const unsigned long long by = speed_bits(face_speed<T, true>(cprev[k], cur[k]));
-                                    if (by > *cbest) *cbest = by;
-                                }
-                            }
-                        }
-                    }
-#pragma unroll
-                    for (int k = 0; k < CPT; ++k) {
-                        cprev[k] = cur[k];
-                        mprev[k] = mcur[k];
-                    }
                 }
             }
 
@@ -1042,10 +891,6 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
                 e4[k] = e3[k]; xe4[k] = xe3[k]; fn4[k] = Fy[k];
                 zbp6[k] = zbp5[k]; zbp5[k] = zbp4[k];
                 gg6[k] = gg5[k]; gg5[k] = gg4[k];
-                if constexpr (CFL) {
-                    f2h[k] = f1h[k]; f2u[k] = f1u[k]; f2v[k] = f1v[k];
-                    f1h[k] = fqh[k]; f1u[k] = fqu[k]; f1v[k] = fqv[k];
-                }
             }
         };
         const int steady0 = min(L0 + 5, L1), steady1 = L1;
@@ -1076,49 +921,26 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
 // warp index; further items come from a grid-wide queue (one atomic per item), so warps
 // on lightly loaded SMs take more of them and no SM waits on a fixed share.  The last
 // block to finish resets the queue for the next launch on the stream.
-// CFL: the averaging stage also takes the next step's time step (the largest face speed of
-// its output, see re_stage_item): warp and block maxima, one atomicMax per block before the
-// block's ticket, and the last block finalises dt exactly as re_cfl_kernel does.
-template <class T, bool MPM, bool HAS_MASK, bool AVG, bool BUD = false, bool CFL = false>
+template <class T, bool MPM, bool HAS_MASK, bool AVG, bool BUD = false>
 __global__ void __launch_bounds__(128, PXB_STAGE_BOUNDS(T, AVG)) re_stage_kernel(const REStageArgs<T> a) {
     const int lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     const int nitems = pxb_stage_items_per_band(a.nstrips) * a.nbands;
     bool bad = false;
-    unsigned long long best = 0ull;
     int item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     while (item < nitems) {
-        re_stage_item<T, MPM, HAS_MASK, AVG, BUD, CFL>(a, item, bad, &best);
+        re_stage_item<T, MPM, HAS_MASK, AVG, BUD>(a, item, bad);
         unsigned next = 0;
         if (lane == 0) next = atomicAdd(&a.queue[0], 1u);
         item = nw + (int)__shfl_sync(FULL, next, 0);
     }
     if (bad) atomicOr(a.err, 1);
-    __shared__ unsigned long long wmax[CFL ? 4 : 1];
-    if constexpr (CFL) {
-        for (int o = 16; o > 0; o >>= 1) {
-            const unsigned long long other = __shfl_xor_sync(FULL, best, o);
-            best = other > best ? other : best;
-        }
-        if (lane == 0) wmax[threadIdx.x >> 5] = best;
-    }
     __syncthreads();
     if (threadIdx.x == 0) {
-        if constexpr (CFL) {
-#pragma unroll
-            for (int w = 1; w < 4; ++w) best = wmax[w] > best ? wmax[w] : best;
-            if (best != 0ull) atomicMax(&a.cscr->maxbits, best);
-        }
-        __threadfence();  // the block's results (and maximum) before its ticket
+        __threadfence();
         if (atomicAdd(&a.queue[1], 1u) == gridDim.x - 1) {
             atomicExch(&a.queue[0], 0u);
             atomicExch(&a.queue[1], 0u);
-            if constexpr (CFL) {
-                __threadfence();
-                cfl_finalize<T>(a.cscr, atomicAdd(&a.cscr->maxbits, 0ull), a.cfl, a.dx, a.cfl_floor, a.cfl_dt_out,
-                                a.cfl_dt_log);
-                __threadfence();
-            }
         }
     }
 }

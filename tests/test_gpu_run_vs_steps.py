@@ -1,14 +1,11 @@
-"""The SSPRK2 run loop takes each next time step inside the averaging stage (GPU only).
+"""A run of n SSPRK2 steps against n runs of one step (GPU only).
 
-``run_steps(n)`` launches the CFL kernel once, for the first step; every later step's
-dt is the largest face speed of the previous averaging stage's output, reduced by that
-stage kernel as it stores the state (the CFL rule of roe_exner.py:compute_dt and
-integrators.py: dt = cfl * dx / max speed, with the same faces, wet/dry and nodata
-rules).  A run of n single steps takes every dt from the stored state with the CFL
-kernel instead.  The two must give the same dts and the same state bit for bit: the
-fused reduction sees the same values (the averaged output, formed one row and one
-column beyond what the item stores, where its inputs are still exact) and a maximum
-does not depend on the order it is taken in.
+``run_steps(n)`` replays the captured graph of one step (CFL launch, stage 1, averaging
+stage) n times back to back, the stage and CFL work queues and the running speed
+maximum reset by their kernels' last blocks between launches; n runs of one step replay
+it once per call, each with its own dt log.  The two must give the same dts and the
+same state bit for bit on every layout, band height and regime: nothing the kernels
+carry from one launch to the next may leak into the arithmetic.
 """
 import numpy as np
 import pytest
@@ -43,7 +40,7 @@ def device_case(arrs, params, X, Y, dtype, dx=0.1):
     return bundle.init_fn(st, mask, cfg), mask, cfg
 
 
-def fused_vs_single(st, mask, cfg, nsteps):
+def run_vs_single(st, mask, cfg, nsteps):
     from pyexner_b200 import run_steps
 
     a = st.clone()
@@ -71,25 +68,25 @@ def fused_vs_single(st, mask, cfg, nsteps):
     ((300, 530), 0, "fast", "trans_x_refl_y", True),
 ])
 @pytest.mark.parametrize("dtype", [torch.float32, torch.float64], ids=["f32", "f64"])
-def test_fused_next_dt_matches_step_by_step(shape, band_rows, regime, bc, mpm, dtype):
+def test_run_matches_single_steps(shape, band_rows, regime, bc, mpm, dtype):
     """Strips and bands of many sizes (items of one row included: bands of 2 rows whose
-    boundary strips split into halves, so that the row above an item is the last row of
-    another), wet/dry fronts, nodata cells, inflow, MPM and constant grass factors: 10
-    steps in one run against 10 runs of one step."""
+    boundary strips split into halves), wet/dry fronts, nodata cells, inflow, MPM and
+    constant grass factors: 10 steps in one run against 10 runs of one step."""
     ny, nx = shape
     arrs, params, X, Y, mpm = random_re_case(ny, nx, seed=ny * 31 + nx, regime=regime, bcname=bc, mpm=mpm)
     params["band_rows"] = band_rows
     st, mask, cfg = device_case(arrs, params, X, Y, dtype)
-    fused_vs_single(st, mask, cfg, 10)
+    run_vs_single(st, mask, cfg, 10)
 
 
 @pytest.mark.parametrize("dtype", [torch.float32, torch.float64], ids=["f32", "f64"])
 @pytest.mark.parametrize("u0", [0.1, 0.55, 1.0])
-def test_fused_next_dt_gaussian_bed(u0, dtype):
-    """The Gaussian-bed workload below, at and above the Shields threshold (no, part and
-    all of the cells carrying bedload, so both face-speed forms of the reduction run)."""
+def test_run_matches_single_steps_gaussian_bed(u0, dtype):
+    """The Gaussian-bed workload, below, at and above the Shields threshold (no, part and
+    all of the cells carrying bedload, so both face-speed forms of the CFL reduction and
+    both Exner paths of the stage run)."""
     from pyexner_b200 import cases
 
     c = cases.gaussian_bed(254, u0=u0)
     st, mask, cfg = device_case(c["arrs"], c["params"], c["X"], c["Y"], dtype, c["dx"])
-    fused_vs_single(st, mask, cfg, 12)
+    run_vs_single(st, mask, cfg, 12)
