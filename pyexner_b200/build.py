@@ -13,6 +13,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -61,15 +62,19 @@ def build(force=False, verbose=False):
     if not force and up_to_date():
         return LIB
     os.makedirs(BUILD, exist_ok=True)
-    objs = []
+    objs, cmds = [], []
     knobs = os.environ.get("PXB_NVCC_DEFINES", "").split()  # e.g. "-DPXB_STAGE_MIN_BLOCKS=4" for tuning sweeps
     for src, extra in UNITS:
         obj = os.path.join(BUILD, src.replace(".cu", ".o"))
-        cmd = [nvcc(), *ARCH, *COMMON, *extra, *knobs, "-c", os.path.join(CSRC, src), "-o", obj]
-        if verbose:
-            print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
+        cmds.append([nvcc(), *ARCH, *COMMON, *extra, *knobs, "-c", os.path.join(CSRC, src), "-o", obj])
         objs.append(obj)
+    # the translation units are independent: compile them side by side
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as pool:
+        for cmd in cmds:
+            if verbose:
+                print(" ".join(cmd))
+        for f in [pool.submit(subprocess.run, cmd, check=True) for cmd in cmds]:
+            f.result()
     tmp = LIB + ".tmp"
     cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs]
     if verbose:
