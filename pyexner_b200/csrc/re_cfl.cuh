@@ -312,8 +312,16 @@ __device__ __forceinline__ void re_cfl_item(const CflArgs<T>& a, const int item,
   }
 }
 
+// Resident 256-thread blocks per SM the CFL kernel is compiled for (tuning knob; by
+// default the compiler's register choice sets it).
+#ifdef PXB_CFL_MIN_BLOCKS
+#define PXB_CFL_BOUNDS __launch_bounds__(256, PXB_CFL_MIN_BLOCKS)
+#else
+#define PXB_CFL_BOUNDS __launch_bounds__(256)
+#endif
+
 template <class T, bool HAS_MASK>
-__global__ void __launch_bounds__(256) re_cfl_kernel(const CflArgs<T> a) {
+__global__ void PXB_CFL_BOUNDS re_cfl_kernel(const CflArgs<T> a) {
     const int lane = threadIdx.x & 31;
     const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
