@@ -18,20 +18,28 @@ Reported:
   roofline   the stage kernels' algorithmic bytes per launch over their CUDA-event
              duration, against the measured HBM copy bandwidth;
   fp64       the same loop in float64 (the plain FP64 GPU path) and its speed ratio;
-  accuracy   rel-L1 of h and z+z_b, float32 vs float64 after the accuracy run;
-  cpu_baseline  the float64 C/OpenMP oracle (all host threads) on a 512 x 512 sample of
-             the same generator, about 10 s of CPU work;
+  accuracy   after 2000 SSPRK2 steps: rel-L1 and L-inf of h, hu, hv and z+z_b, float32
+             vs float64 on the GPU at 2048^2 and both GPU precisions vs the float64 C
+             oracle at 1024^2, with the volume-budget closure of each GPU run;
+  cpu_baseline  the float32 build of the C/OpenMP restatement of the reference step (all
+             host threads) on the 2048^2 workload itself, steps until about 10 s of CPU
+             work;
   plain_roe  the plain Roe dam-break (256^2, float64, SSPRK2, 200 steps)
              and the NumPy oracle on the host for 10 steps of it;
   transport_case  the same case started at u = 1 m/s (Shields number about 0.15, bedload
              in every cell, so the stage kernel's sediment-free fast path never fires);
   ensemble   the ragged ensemble workload (64 Roe-Exner dam breaks, sides U{128..1024},
              own beds, step heights and dts; float32; 1000 SSPRK2 steps): autotuned band
-             height, cell-updates/s over all members (state ~1.1 GB, larger than L2).
+             height, cell-updates/s over all members (state ~1.1 GB, larger than L2); under
+             torchrun the members are split over the ranks and the rates summed;
+  bandwidth_case  the same generator at 8192^2, K timed steps;
+  adjoint    the configuration-4 inflow case (512^2, float64): forward and checkpointed
+             backward ms per SSPRK2 step with the parameter adjoints.
 
-``--impl reference`` times the reference algorithm on the CPU instead (the float64
-C/OpenMP restatement of PyExner's JAX step, oracle/c; JAX itself is not installed on
-these hosts) and prints its line with "impl": "reference".
+``--impl reference`` times the reference algorithm on the CPU instead (the float32 build
+of the C/OpenMP restatement of PyExner's JAX step, oracle/c, on the 2048^2 workload, the
+float64 build timed beside it; JAX itself is not installed on these hosts) and prints its
+line with "impl": "reference".
 """
 from __future__ import annotations
 
