@@ -147,6 +147,21 @@ typedef struct pxb_re_config {
 int pxb_re_plan_create(const pxb_re_config* cfg, pxb_re_plan** out);
 int pxb_re_plan_destroy(pxb_re_plan* plan);
 
+/* Caller-owned device memory (the workspace of the plan-and-buffers ownership model: the host
+ * framework owns every device buffer, the library allocates none).  *bytes receives the device
+ * bytes a plan for cfg needs: its boundary tables and scratch, and on the general stage path
+ * its seven scratch planes.  pxb_re_plan_create_in builds the same plan inside `workspace` (a
+ * device pointer, 256-byte aligned, at least that many bytes, untouched by the caller until
+ * pxb_re_plan_destroy): its creation and its pxb_re_init, pxb_re_cfl, pxb_re_stage,
+ * pxb_re_volume, pxb_re_autotune and pxb_re_check calls allocate no device memory.
+ * pxb_re_run captures its step graph on first use, which the CUDA driver allocates for;
+ * pxb_re_set_budget, the tangent-linear model (pxb_re_jvp_*) and the reverse mode
+ * (pxb_re_vjp_*), which allocate their tables on first use, return PXB_ERR_UNSUPPORTED on
+ * such a plan.  Replaces the plans' cudaMalloc of their tables (no counterpart in the
+ * reference, whose JAX arrays are allocated by XLA: solvers/roe_exner_solver.py:58-122). */
+int pxb_re_plan_workspace_size(const pxb_re_config* cfg, size_t* bytes);
+int pxb_re_plan_create_in(const pxb_re_config* cfg, void* workspace, size_t bytes, pxb_re_plan** out);
+
 /* init_fn_roeexner (roe_exner_solver.py:58-78): n_b, G, then the handlers at t = 0, in place. */
 int pxb_re_init(pxb_re_plan* plan, const pxb_re_fields* f, void* stream);
 

@@ -8,7 +8,7 @@ from __future__ import annotations
 import ctypes
 import os
 import re
-from ctypes import POINTER, c_double, c_int, c_int32, c_int64, c_void_p
+from ctypes import POINTER, c_double, c_int, c_int32, c_int64, c_size_t, c_void_p
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libpyexner_b200.so")
@@ -131,6 +131,8 @@ _lib = None
 SIGNATURES = {
     "pxb_re_plan_create": [POINTER(REConfig), POINTER(c_void_p)],
     "pxb_re_plan_destroy": [c_void_p],
+    "pxb_re_plan_workspace_size": [POINTER(REConfig), POINTER(c_size_t)],
+    "pxb_re_plan_create_in": [POINTER(REConfig), c_void_p, c_size_t, POINTER(c_void_p)],
     "pxb_re_init": [c_void_p, POINTER(REFields), c_void_p],
     "pxb_re_plan_path": [c_void_p],
     "pxb_re_autotune": [c_void_p, POINTER(REFields), POINTER(REFields), c_void_p, POINTER(c_int32)],

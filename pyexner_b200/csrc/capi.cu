@@ -361,8 +361,39 @@ Geometry cfl_geometry(int ny, int nx, int resident_warps) {
     return g;
 }
 
+// Device memory of a plan: cudaMalloc'd (no arena), carved from a caller's workspace, or
+// only counted (the size query of pxb_re_plan_workspace_size).  Carved blocks start on
+// 256-byte boundaries.
+struct DevArena {
+    char* base = nullptr;  // the caller's workspace (carving), null when counting
+    size_t cap = 0, used = 0;
+    bool counting = false;
+};
+
+int arena_alloc(DevArena* A, void** p, size_t bytes, const char* what) {
+    *p = nullptr;
+    if (!A) {
+        const cudaError_t e = cudaMalloc(p, bytes);
+        if (e != cudaSuccess) return fail(PXB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+        return PXB_OK;
+    }
+    const size_t at = (A->used + 255) & ~(size_t)255;
+    A->used = at + bytes;
+    if (A->counting) return PXB_OK;
+    if (A->used > A->cap) return fail(PXB_ERR_ARG, std::string("workspace too small (") + what + ")");
+    *p = A->base + at;
+    return PXB_OK;
+}
+
+// Host -> device copy unless the arena only counts.
+int arena_copy(DevArena* A, void* dst, const void* src, size_t bytes) {
+    if (A && A->counting) return PXB_OK;
+    PXB_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+    return PXB_OK;
+}
+
 int upload_handlers(const pxb_bc_handler* hs, int nh, long long max_index, std::vector<DevHandler>& out,
-                    int& maxcount) {
+                    int& maxcount, DevArena* A = nullptr) {
     maxcount = 0;
     for (int k = 0; k < nh; ++k) {
         const pxb_bc_handler& H = hs[k];
@@ -405,10 +436,15 @@ int upload_handlers(const pxb_bc_handler* hs, int nh, long long max_index, std::
                 break;
         }
         if (H.count > 0) {
-            PXB_CUDA(cudaMalloc(&d.cells, sizeof(long long) * H.count));
-            PXB_CUDA(cudaMalloc(&d.donors, sizeof(long long) * H.count));
-            PXB_CUDA(cudaMemcpy(d.cells, H.cells, sizeof(long long) * H.count, cudaMemcpyHostToDevice));
-            PXB_CUDA(cudaMemcpy(d.donors, H.donors, sizeof(long long) * H.count, cudaMemcpyHostToDevice));
+            const size_t nb = sizeof(long long) * H.count;
+            int st = arena_alloc(A, (void**)&d.cells, nb, "boundary cells");
+            if (st == PXB_OK) st = arena_alloc(A, (void**)&d.donors, nb, "boundary donors");
+            if (st == PXB_OK) st = arena_copy(A, d.cells, H.cells, nb);
+            if (st == PXB_OK) st = arena_copy(A, d.donors, H.donors, nb);
+            if (st != PXB_OK) {
+                out.push_back(d);  // released with the plan
+                return st;
+            }
         }
         maxcount = std::max(maxcount, H.count);
         out.push_back(d);
@@ -484,7 +520,8 @@ struct PlanCommon {
     void* bc_tmp = nullptr;
     pxb::CflScratch* scr = nullptr;
     void* dt_dev = nullptr;
-    cudaStream_t cap = nullptr;
+    cudaStream_t cap = nullptr;  // capture stream of the graph cache, created on first use
+    bool ws = false;             // device memory carved from the caller's workspace
     Geometry cfl;
     // graph cache
     struct Cached {
@@ -497,16 +534,18 @@ struct PlanCommon {
 
     void release() {
         for (auto& h : handlers) {
-            cudaFree(h.cells);
-            cudaFree(h.donors);
+            if (!ws) cudaFree(h.cells);
+            if (!ws) cudaFree(h.donors);
         }
         handlers.clear();
         for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
         graphs.clear();
-        cudaFree(ring);
-        cudaFree(bc_tmp);
-        cudaFree(scr);
-        cudaFree(dt_dev);
+        if (!ws) {
+            cudaFree(ring);
+            cudaFree(bc_tmp);
+            cudaFree(scr);
+            cudaFree(dt_dev);
+        }
         if (cap) cudaStreamDestroy(cap);
         ring = nullptr;
         bc_tmp = nullptr;
@@ -525,7 +564,7 @@ bool kind_ok(int kind, bool roe) {
 
 // want_path: PXB_PATH_AUTO / _FUSED / _GENERAL (Roe plans: fused only); path: the result.
 int common_setup(PlanCommon& P, int ny, int nx, long long pitch, int dtype, double dx, const pxb_bc_handler* hs,
-                 int nh, bool roe, int want_path, int& path) {
+                 int nh, bool roe, int want_path, int& path, DevArena* A = nullptr) {
     if (ny < 3 || nx < 3) return fail(PXB_ERR_ARG, "grid must be at least 3 x 3 cells including the ring");
     if (pitch < nx) return fail(PXB_ERR_ARG, "pitch smaller than nx");
     if ((long long)ny * pitch >= (1LL << 31)) return fail(PXB_ERR_ARG, "planes of 2^31 elements or more are not supported");
@@ -547,28 +586,33 @@ int common_setup(PlanCommon& P, int ny, int nx, long long pitch, int dtype, doub
             return fail(PXB_ERR_ARG, "boundary handler " + std::to_string(k) + " has kind " + std::to_string(hs[k].kind) +
                                          (roe ? ", not a \"Roe\" handler" : ", not a \"Roe Exner\" handler"));
     path = want_path == PXB_PATH_GENERAL ? PXB_PATH_GENERAL : PXB_PATH_FUSED;
+    P.ws = A != nullptr;
     if (nh > 0) {
         int maxcount = 0;
-        int st = upload_handlers(hs, nh, (long long)(ny - 1) * pitch + nx, P.handlers, maxcount);
+        int st = upload_handlers(hs, nh, (long long)(ny - 1) * pitch + nx, P.handlers, maxcount, A);
         if (st != PXB_OK) return st;
-        PXB_CUDA(cudaMalloc(&P.bc_tmp, 6 * (size_t)std::max(1, maxcount) * P.esize()));
+        st = arena_alloc(A, &P.bc_tmp, 6 * (size_t)std::max(1, maxcount) * P.esize(), "boundary scratch");
+        if (st != PXB_OK) return st;
         if (path == PXB_PATH_FUSED) {
             Resolved R = resolve(hs, nh, ny, nx, pitch, roe, !roe);
             if (!R.error.empty()) {
                 if (want_path == PXB_PATH_FUSED || roe) return fail(PXB_ERR_UNSUPPORTED, R.error);
                 path = PXB_PATH_GENERAL;
             } else {
-                PXB_CUDA(cudaMalloc(&P.ring, sizeof(pxb_ring_recipe) * R.ring.size()));
-                PXB_CUDA(cudaMemcpy(P.ring, R.ring.data(), sizeof(pxb_ring_recipe) * R.ring.size(),
-                                    cudaMemcpyHostToDevice));
+                const size_t nb = sizeof(pxb_ring_recipe) * R.ring.size();
+                st = arena_alloc(A, (void**)&P.ring, nb, "ring recipes");
+                if (st == PXB_OK) st = arena_copy(A, P.ring, R.ring.data(), nb);
+                if (st != PXB_OK) return st;
             }
         }
     }
-    PXB_CUDA(cudaMalloc(&P.scr, sizeof(pxb::CflScratch)));
-    PXB_CUDA(cudaMemset(P.scr, 0, sizeof(pxb::CflScratch)));
-    PXB_CUDA(cudaMalloc(&P.dt_dev, 8));
-    PXB_CUDA(cudaMemset(P.dt_dev, 0, 8));
-    PXB_CUDA(cudaStreamCreateWithFlags(&P.cap, cudaStreamNonBlocking));
+    int st = arena_alloc(A, (void**)&P.scr, sizeof(pxb::CflScratch), "scratch");
+    if (st == PXB_OK) st = arena_alloc(A, &P.dt_dev, 8, "time step");
+    if (st != PXB_OK) return st;
+    if (!(A && A->counting)) {
+        PXB_CUDA(cudaMemset(P.scr, 0, sizeof(pxb::CflScratch)));
+        PXB_CUDA(cudaMemset(P.dt_dev, 0, 8));
+    }
     return PXB_OK;
 }
 
@@ -593,6 +637,7 @@ int run_graph(PlanCommon& P, const std::vector<const void*>& key, int reps, cuda
         if (g.key == key) exec = g.exec;
     if (!exec) {
         cudaGraph_t graph;
+        if (!P.cap) PXB_CUDA(cudaStreamCreateWithFlags(&P.cap, cudaStreamNonBlocking));
         PXB_CUDA(cudaStreamBeginCapture(P.cap, cudaStreamCaptureModeThreadLocal));
         const int st = body(P.cap);
         cudaGraph_t tmp = nullptr;
@@ -2068,20 +2113,24 @@ int pxb_label_polygons(int32_t ny, int32_t nx, const double* xc, const double* y
 }
 int pxb_version(void) { return 1; }
 
-int pxb_re_plan_create(const pxb_re_config* cfg, pxb_re_plan** out) {
+namespace {
+// Roe-Exner plan on cudaMalloc'd memory (A null), on the caller's workspace, or only
+// counting the workspace's size (A->counting; the plan is then discarded).
+int re_plan_create(const pxb_re_config* cfg, DevArena* A, pxb_re_plan** out) {
     if (!cfg || !out) return fail(PXB_ERR_ARG, "null config or output pointer");
     *out = nullptr;
     if (cfg->mpm && (!cfg->seds || cfg->nsed < 1 || cfg->nsed > PXB_MAX_SED))
         return fail(PXB_ERR_ARG, "MPM needs 1..8 sediment classes");
     pxb_re_plan* P = new pxb_re_plan();
     int st = common_setup(P->c, cfg->ny, cfg->nx, cfg->pitch, cfg->dtype, cfg->dx, cfg->handlers, cfg->nhandlers, false,
-                          cfg->stage_path, P->path);
-    if (st == PXB_OK && P->path == PXB_PATH_GENERAL) {
-        const cudaError_t e = cudaMalloc(&P->gen, 7 * (size_t)cfg->ny * (size_t)cfg->pitch * P->c.esize());
-        if (e != cudaSuccess) st = fail(PXB_ERR_CUDA, std::string("scratch planes: ") + cudaGetErrorString(e));
-    }
-    if (st != PXB_OK) {
-        cudaFree(P->gen);
+                          cfg->stage_path, P->path, A);
+    if (st == PXB_OK && P->path == PXB_PATH_GENERAL)
+        st = arena_alloc(A, &P->gen, 7 * (size_t)cfg->ny * (size_t)cfg->pitch * P->c.esize(), "scratch planes");
+    if (st == PXB_OK && A)  // the volume reduction's block partials (allocated on first use otherwise)
+        st = arena_alloc(A, (void**)&P->vol_scr, sizeof(double) * (4 * (size_t)(4 * P->c.sm_count) + 2),
+                         "volume scratch");
+    if (st != PXB_OK || (A && A->counting)) {
+        if (!P->c.ws) cudaFree(P->gen);
         P->c.release();
         delete P;
         return st;
@@ -2110,16 +2159,48 @@ int pxb_re_plan_create(const pxb_re_config* cfg, pxb_re_plan** out) {
     return PXB_OK;
 }
 
+// Entry points that allocate device tables on first use refuse a workspace plan.
+int refuse_ws(const pxb_re_plan* P, const char* what) {
+    if (P && P->c.ws)
+        return fail(PXB_ERR_UNSUPPORTED, std::string(what) + " allocates device memory: not on a workspace plan");
+    return PXB_OK;
+}
+}  // namespace
+
+int pxb_re_plan_create(const pxb_re_config* cfg, pxb_re_plan** out) { return re_plan_create(cfg, nullptr, out); }
+
+int pxb_re_plan_workspace_size(const pxb_re_config* cfg, size_t* bytes) {
+    if (!bytes) return fail(PXB_ERR_ARG, "null output pointer");
+    *bytes = 0;
+    DevArena A;
+    A.counting = true;
+    pxb_re_plan* P = nullptr;
+    const int st = re_plan_create(cfg, &A, &P);
+    if (st != PXB_OK) return st;
+    *bytes = A.used;
+    return PXB_OK;
+}
+
+int pxb_re_plan_create_in(const pxb_re_config* cfg, void* workspace, size_t bytes, pxb_re_plan** out) {
+    if (!workspace || ((uintptr_t)workspace & 255u)) return fail(PXB_ERR_ARG, "workspace must be 256-byte aligned");
+    DevArena A;
+    A.base = (char*)workspace;
+    A.cap = bytes;
+    return re_plan_create(cfg, &A, out);
+}
+
 int pxb_re_plan_destroy(pxb_re_plan* plan) {
     if (!plan) return PXB_OK;
     cudaDeviceSynchronize();
     plan->c.release();
-    cudaFree(plan->gen);
+    if (!plan->c.ws) {
+        cudaFree(plan->gen);
+        cudaFree(plan->vol_scr);
+    }
     cudaFree(plan->jvp);
     cudaFree(plan->dscr);
     cudaFree(plan->jvp_tmp);
     cudaFree(plan->bud_part);
-    cudaFree(plan->vol_scr);
     delete plan;
     return PXB_OK;
 }
@@ -2195,6 +2276,10 @@ int pxb_re_run(pxb_re_plan* P, const pxb_re_fields* a, const pxb_re_fields* b, i
 
 int pxb_re_set_budget(pxb_re_plan* P, double* acc_dev) {
     if (!P) return fail(PXB_ERR_ARG, "null plan");
+    if (acc_dev && !P->bud_part) {
+        const int st = refuse_ws(P, "the volume budget");
+        if (st != PXB_OK) return st;
+    }
     if (acc_dev && P->path != PXB_PATH_FUSED)
         return fail(PXB_ERR_UNSUPPORTED, "the volume budget is built into the fused stage path only");
     if (acc_dev && ((uintptr_t)acc_dev & 7u)) return fail(PXB_ERR_ARG, "acc_dev must be 8-byte aligned");
@@ -2233,6 +2318,7 @@ int pxb_re_volume(pxb_re_plan* P, const pxb_re_fields* f, double* volumes, void*
 int pxb_re_jvp_init(pxb_re_plan* P, const pxb_re_fields* f, const pxb_re_fields* f_dot,
                     const pxb_re_tangent_params* tp, void* stream) {
     if (!P) return fail(PXB_ERR_ARG, "null plan");
+    if (refuse_ws(P, "the tangent-linear model") != PXB_OK) return PXB_ERR_UNSUPPORTED;
     if (P->c.dtype != PXB_F64) return fail(PXB_ERR_ARG, "the tangent-linear model runs on float64 plans");
     int st = check_tangent_fields(f, "state");
     if (st == PXB_OK) st = check_tangent_fields(f_dot, "tangent");
@@ -2247,6 +2333,7 @@ int pxb_re_jvp_run(pxb_re_plan* P, const pxb_re_fields* a, const pxb_re_fields* 
                    double cfl, double t0, const pxb_re_tangent_params* tp, void* dt_log, void* dt_dot_log,
                    void* stream) {
     if (!P) return fail(PXB_ERR_ARG, "null plan");
+    if (refuse_ws(P, "the tangent-linear model") != PXB_OK) return PXB_ERR_UNSUPPORTED;
     if (P->c.dtype != PXB_F64) return fail(PXB_ERR_ARG, "the tangent-linear model runs on float64 plans");
     int st = check_tangent_fields(a, "state");
     if (st == PXB_OK) st = check_tangent_fields(a_dot, "tangent");
@@ -2264,6 +2351,7 @@ int pxb_re_jvp_run(pxb_re_plan* P, const pxb_re_fields* a, const pxb_re_fields* 
 int pxb_re_vjp_init_params(pxb_re_plan* P, const pxb_re_fields* f, const pxb_re_fields* fbar,
                            const pxb_re_param_adjoints* pbar, void* stream) {
     if (!P) return fail(PXB_ERR_ARG, "null plan");
+    if (refuse_ws(P, "the reverse mode") != PXB_OK) return PXB_ERR_UNSUPPORTED;
     if (P->c.dtype != PXB_F64) return fail(PXB_ERR_ARG, "the reverse mode runs on float64 plans");
     if (!f || !f->h || !f->hu || !f->hv) return fail(PXB_ERR_ARG, "state: h, hu and hv must be set");
     if (!fbar || !fbar->h || !fbar->hu || !fbar->hv || !fbar->z_b || !fbar->G)
@@ -2285,6 +2373,7 @@ int pxb_re_vjp_run_params(pxb_re_plan* P, const pxb_re_fields* a0, int32_t nstep
                           double t0, int32_t checkpoint_every, const pxb_re_fields* abar,
                           const pxb_re_param_adjoints* pbar, void* stream) {
     if (!P) return fail(PXB_ERR_ARG, "null plan");
+    if (refuse_ws(P, "the reverse mode") != PXB_OK) return PXB_ERR_UNSUPPORTED;
     if (P->c.dtype != PXB_F64) return fail(PXB_ERR_ARG, "the reverse mode runs on float64 plans");
     if (!a0 || !a0->h || !a0->hu || !a0->hv || !a0->z || !a0->z_b || !a0->n_b || !a0->G)
         return fail(PXB_ERR_ARG, "state: h, hu, hv, z, z_b, n_b and G must be set");

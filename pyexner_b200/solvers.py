@@ -86,9 +86,12 @@ def _dtype_code(t):
 
 # ============================================================== Roe Exner
 class RePlan:
-    """Owner of one ``pxb_re_plan`` (boundary recipes, CFL scratch, graphs)."""
+    """Owner of one ``pxb_re_plan`` (boundary recipes, CFL scratch, graphs).
 
-    def __init__(self, state, mask, config, band_rows=0, stage_path=0):
+    ``workspace=True``: the plan's device memory is a torch tensor this object holds
+    (``pxb_re_plan_create_in``), so the library allocates none for it."""
+
+    def __init__(self, state, mask, config, band_rows=0, stage_path=0, workspace=False):
         ny, nx = state.shape
         self.mpm = isinstance(config.compute_G, str)
         nod = None
@@ -115,7 +118,16 @@ class RePlan:
         cfg.band_rows = int(band_rows)
         cfg.stage_path = int(stage_path)
         h = ctypes.c_void_p()
-        _lib.call("pxb_re_plan_create", ctypes.byref(cfg), ctypes.byref(h))
+        self.workspace = None
+        if workspace:
+            size = ctypes.c_size_t()
+            _lib.call("pxb_re_plan_workspace_size", ctypes.byref(cfg), ctypes.byref(size))
+            # blocks of torch's caching allocator start on 512-byte boundaries
+            self.workspace = torch.empty(max(1, size.value), dtype=torch.uint8, device=state.h.device)
+            _lib.call("pxb_re_plan_create_in", ctypes.byref(cfg), ctypes.c_void_p(self.workspace.data_ptr()),
+                      ctypes.c_size_t(self.workspace.numel()), ctypes.byref(h))
+        else:
+            _lib.call("pxb_re_plan_create", ctypes.byref(cfg), ctypes.byref(h))
         self.handle = h
         self.path = _lib.load().pxb_re_plan_path(h)
         self.dtype = state.dtype
