@@ -201,7 +201,18 @@ __device__ __forceinline__ void read_cols(const T* rowp, int lane, T (&v)[CPT]) 
 // consecutive columns (pxb_stage_cpt): a strip is 32 * CPT columns, 3 halo | owned | 3
 // halo.  Neighbour values inside a lane are plain registers; across lanes one shuffle
 // moves the first (east) or last (west) column.
-template <class T, bool MPM, bool HAS_MASK, bool AVG, bool BUD = false>
+// A block's shared buffer of the stage kernel (TAG: 0 row copies, 1 partner copies),
+// one object for every instantiation of re_stage_item with these dimensions, so that
+// the interior and the boundary instantiations in one kernel share it.
+template <class T, int TAG, int D0, int D1, int D2, int D3>
+__device__ __forceinline__ T (&stage_smem())[D0][D1][D2][D3] {
+    __shared__ __align__(16) T buf[D0][D1][D2][D3];
+    return buf;
+}
+
+// INTERIOR: the instantiation for items away from the grid's boundary (no boundary strip
+// or row), which carries none of the boundary-recipe code.
+template <class T, bool MPM, bool HAS_MASK, bool AVG, bool BUD = false, bool INTERIOR = false>
 __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int item, bool& bad) {
     constexpr int CPT = pxb_stage_cpt((int)sizeof(T));
     constexpr int W = 32 * CPT;
@@ -220,16 +231,19 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
         if (ipb == 1) strip = 0;
         else if (kb < 2) { strip = 0; half = kb; }
         else if (kb >= a.nstrips) { strip = a.nstrips - 1; half = kb - a.nstrips; }
-        const bool last_strip = strip == a.nstrips - 1;
+        const bool last_strip = !INTERIOR && strip == a.nstrips - 1;
         const int cb = strip * (W - 2 * PXB_HALO) - PXB_HALO + CPT * lane;  // column of this lane's first element
         bool colok[CPT], has_e[CPT], out_col[CPT], interior_col[CPT];
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
             const int c = cb + k, j = CPT * lane + k;
-            colok[k] = (c >= 0) && (c < nx);
-            has_e[k] = colok[k] && (c + 1 < nx) && (j < W - 1);
+            // an interior strip lies inside the grid's columns 1 .. nx-2 (it is neither the
+            // first nor the last strip, and every strip but the last ends two columns
+            // short of column nx - 1)
+            colok[k] = INTERIOR || ((c >= 0) && (c < nx));
+            has_e[k] = colok[k] && (INTERIOR || c + 1 < nx) && (j < W - 1);
             out_col[k] = colok[k] && j >= PXB_HALO && (j < W - PXB_HALO || last_strip);
-            interior_col[k] = (c >= 1) && (c <= nx - 2);
+            interior_col[k] = INTERIOR || ((c >= 1) && (c <= nx - 2));
         }
         const int B0 = band * a.band_rows;
         const int B1 = (band == a.nbands - 1) ? ny : B0 + a.band_rows;
@@ -238,8 +252,8 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
         const int R1 = half == 0 ? Bm : B1;
         const int L0 = max(0, R0 - 3), L1 = min(ny, R1 + 3);
         // boundary recipes can only apply in the first/last strip or on rows 0 / ny-1
-        const bool bc_strip = (a.ring != nullptr) && (strip == 0 || last_strip);
-        const bool bc_rows = (a.ring != nullptr) && (R0 == 0 || R1 == ny);
+        const bool bc_strip = !INTERIOR && (a.ring != nullptr) && (strip == 0 || last_strip);
+        const bool bc_rows = !INTERIOR && (a.ring != nullptr) && (R0 == 0 || R1 == ny);
         // Budget: only items that own boundary faces of physical cells add to the lane slots.
         // A face counts once: in the item that owns its row (x-faces; y-faces (r-1|r) by row
         // r) and, for columns, by the lane that owns the column.  The outflow of a face with
@@ -289,7 +303,7 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
         // float64 (measured: faster there) plain loads into registers.
         constexpr bool ASYNC_ROWS = is_f32<T>();
         constexpr int NP = MPM ? 6 : 7;
-        __shared__ __align__(16) T rbuf[4][ASYNC_ROWS ? 2 : 1][ASYNC_ROWS ? NP : 1][ASYNC_ROWS ? W : 1];
+        auto& rbuf = stage_smem<T, 0, 4, ASYNC_ROWS ? 2 : 1, ASYNC_ROWS ? NP : 1, ASYNC_ROWS ? W : 1>();
         T(*rb)[ASYNC_ROWS ? NP : 1][ASYNC_ROWS ? W : 1] = rbuf[threadIdx.x >> 5];
         T nh[CPT], nhu[CPT], nhv[CPT], nzb[CPT], nz[CPT], nnb[CPT], ng[CPT];
         bool nm[CPT];
@@ -346,7 +360,7 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
         // reads and then writes these cells, so both are safe when the output aliases the
         // partner.
         constexpr bool ASYNC_PARTNER = AVG && is_f32<T>();
-        __shared__ __align__(16) T pbuf[4][ASYNC_PARTNER ? 2 : 1][5][ASYNC_PARTNER ? W : 1];
+        auto& pbuf = stage_smem<T, 1, 4, ASYNC_PARTNER ? 2 : 1, 5, ASYNC_PARTNER ? W : 1>();
         T(*pb)[5][ASYNC_PARTNER ? W : 1] = pbuf[threadIdx.x >> 5];
         auto partner_copy = [&](const int rr) __attribute__((always_inline)) {  // the rows stored in iteration rr
             const int q0 = rr - 3, p0 = rr - 5;
@@ -377,7 +391,7 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
         // read theirs directly.  The first application leaves the z_b / G fields of the
         // second (row p = r-5, two iterations later) in a packed word.  Float32 only, as
         // the row copies.
-        constexpr bool ASYNC_RECIPES = ASYNC_ROWS;
+        constexpr bool ASYNC_RECIPES = ASYNC_ROWS && !INTERIOR;
         __shared__ __align__(16) pxb_ring_recipe rcbuf[4][ASYNC_RECIPES ? 2 : 1][2];
         __shared__ unsigned zgbuf[4][ASYNC_RECIPES ? 4 : 1][ASYNC_RECIPES ? W : 1];
         pxb_ring_recipe(*rcb)[2] = rcbuf[threadIdx.x >> 5];
@@ -917,6 +931,18 @@ __device__ __forceinline__ void re_stage_item(const REStageArgs<T>& a, const int
     }
 }
 
+// Whether an item lies away from the grid's boundary: an interior strip (boundary strips
+// are the first two and the last two items of a band, as half-height items) of an
+// interior band, or any item of a grid without boundary recipes.  Such items take the
+// re_stage_item instantiation without boundary code, whose columns are all inside the
+// grid (the same bits, fewer instructions per row).
+template <class T>
+__device__ __forceinline__ bool stage_item_interior(const REStageArgs<T>& a, const int item) {
+    const int ipb = pxb_stage_items_per_band(a.nstrips);
+    const int band = item / ipb, kb = item - band * ipb;
+    return a.ring == nullptr || (ipb > 1 && kb >= 2 && kb < a.nstrips && band > 0 && band < a.nbands - 1);
+}
+
 // The grid is sized to the resident capacity of the device.  A warp's first item is its
 // warp index; further items come from a grid-wide queue (one atomic per item), so warps
 // on lightly loaded SMs take more of them and no SM waits on a fixed share.  The last
@@ -929,7 +955,8 @@ __global__ void __launch_bounds__(128, PXB_STAGE_BOUNDS(T, AVG)) re_stage_kernel
     bool bad = false;
     int item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     while (item < nitems) {
-        re_stage_item<T, MPM, HAS_MASK, AVG, BUD>(a, item, bad);
+        if (stage_item_interior(a, item)) re_stage_item<T, MPM, HAS_MASK, AVG, BUD, true>(a, item, bad);
+        else re_stage_item<T, MPM, HAS_MASK, AVG, BUD, false>(a, item, bad);
         unsigned next = 0;
         if (lane == 0) next = atomicAdd(&a.queue[0], 1u);
         item = nw + (int)__shfl_sync(FULL, next, 0);
