@@ -943,6 +943,21 @@ __device__ __forceinline__ bool stage_item_interior(const REStageArgs<T>& a, con
     return a.ring == nullptr || (ipb > 1 && kb >= 2 && kb < a.nstrips && band > 0 && band < a.nbands - 1);
 }
 
+// Work-queue order of the items: those that run the generic instantiation (the first and
+// the last band, then in every band its boundary strips) come first, so that the items
+// handed out last, which set the kernel's tail, are the uniform interior ones.  A
+// permutation of the item numbers: the results do not depend on it.
+template <class T>
+__device__ __forceinline__ int stage_item_order(const REStageArgs<T>& a, const int q) {
+    const int ipb = pxb_stage_items_per_band(a.nstrips);
+    const int bq = q / ipb, k = q - bq * ipb;
+    const int nb = a.nbands;
+    const int band = (nb < 2 || bq == 0) ? 0 : (bq == 1 ? nb - 1 : bq - 1);
+    // boundary items of a band: kb 0, 1 (first strip) and ipb-2, ipb-1 (last strip)
+    const int kb = (ipb < 4 || k < 2) ? k : (k < 4 ? ipb - 4 + k : k - 2);
+    return band * ipb + kb;
+}
+
 // The grid is sized to the resident capacity of the device.  A warp's first item is its
 // warp index; further items come from a grid-wide queue (one atomic per item), so warps
 // on lightly loaded SMs take more of them and no SM waits on a fixed share.  The last
@@ -955,8 +970,9 @@ __global__ void __launch_bounds__(128, PXB_STAGE_BOUNDS(T, AVG)) re_stage_kernel
     bool bad = false;
     int item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     while (item < nitems) {
-        if (stage_item_interior(a, item)) re_stage_item<T, MPM, HAS_MASK, AVG, BUD, true>(a, item, bad);
-        else re_stage_item<T, MPM, HAS_MASK, AVG, BUD, false>(a, item, bad);
+        const int it = stage_item_order(a, item);
+        if (stage_item_interior(a, it)) re_stage_item<T, MPM, HAS_MASK, AVG, BUD, true>(a, it, bad);
+        else re_stage_item<T, MPM, HAS_MASK, AVG, BUD, false>(a, it, bad);
         unsigned next = 0;
         if (lane == 0) next = atomicAdd(&a.queue[0], 1u);
         item = nw + (int)__shfl_sync(FULL, next, 0);
